@@ -1,0 +1,197 @@
+/*
+ * csg.h — C ABI of the B200 parallel-tempering engine for the 3D +-J
+ * Edwards-Anderson spin glass (libcsg.so).
+ *
+ * The reference program (Marco-Mendivil-Carboni/Spin-Glass) has no library
+ * interface; its boundary is the `csg <sim_dir> <H>` command and the host
+ * class `eamsim` (Program/src/eamsim.cuh:66-110).  Each entry point below
+ * names the member or kernel of that class it replaces.  Conventions:
+ *   - every function returns CSG_OK (0) or a CSG_ERR_* code; the message of
+ *     the last failure on the calling thread is csg_last_error();
+ *   - no exception, exit() or abort() crosses this boundary;
+ *   - an engine owns its device memory; callers own every host buffer;
+ *   - an engine is driven by one host thread and runs on one CUDA stream.
+ *
+ * Layouts (host and device, "canonical"):
+ *   spins  uint32 [W][C][T/4][N][4]  — W words of 32 disorder samples (bit b
+ *          of a word is sample 32w+b), C copies, T temperatures grouped in
+ *          quads, N = L^3 sites in checkerboard order
+ *          slot(x,y,z) = ((x+y+z)&1)*N/2 + ((z*L+y)*(L/2) + x/2),
+ *          innermost axis t%4.  Bit 1 = spin up.
+ *   bonds  uint32 [W][3][N] — bond between slot(i) and i+e_d, d = x,y,z;
+ *          bit 1 = antiferromagnetic (J = -1).  Copies share bonds.
+ */
+#ifndef CSG_H
+#define CSG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    CSG_OK = 0,
+    CSG_ERR_ARG = 1,         /* invalid argument or configuration */
+    CSG_ERR_CUDA = 2,        /* CUDA runtime failure */
+    CSG_ERR_UNSUPPORTED = 3, /* configuration outside what the kernels cover */
+    CSG_ERR_STATE = 4,       /* inconsistent input state (e.g. checkpoint) */
+    CSG_ERR_NOMEM = 5        /* device or host allocation failed */
+};
+
+typedef struct csg_dims {
+    int32_t L;        /* lattice side: even, 4..24 */
+    int32_t n_words;  /* disorder samples / 32 */
+    int32_t n_copies; /* independent copies per sample: 1 or 2 */
+    int32_t n_temps;  /* temperatures: multiple of 4, 4..64 */
+} csg_dims;
+
+typedef struct csg_schedule {
+    int32_t sweeps_per_swap; /* exchange after sweep s when (s+1)%k == 0; 0 = never */
+    int32_t sweeps_per_meas; /* measure after sweep s when (s+1)%k == 0 ... */
+    int64_t meas_start;      /* ... and s >= meas_start; k == 0: never */
+} csg_schedule;
+
+enum {
+    CSG_MEASURE_M = 1 /* also accumulate magnetisations at measurements */
+};
+
+typedef struct csg_config {
+    csg_dims dims;
+    csg_schedule sched;
+    double H;                /* external field, 0 <= H <= 4 (eamsim.cu:520) */
+    uint64_t seed;           /* Philox key of the whole simulation */
+    const double* betas;     /* n_temps inverse temperatures (host); exchanges pair t, t+1 */
+    int32_t flags;           /* CSG_MEASURE_M */
+    int32_t swap_log_rounds; /* keep accepted-exchange masks of this many rounds (tests) */
+} csg_config;
+
+/* Accumulated observables (host arrays; any pointer may be NULL).
+ * Shapes: e/m: [W][C][T][32]; q: [W][T][32]; q4: [W][T][32][2] (128-bit
+ * little-endian halves); hist: [T][N+1] counts of D = #sites where the two
+ * copies differ; swap_acc: [C][T] accepted exchanges of pair (t,t+1);
+ * swap_log: [rounds][W][C][T] accepted-sample masks. */
+typedef struct csg_observables {
+    int64_t* e_sum;
+    int64_t* m_sum;
+    int64_t* q_sum;
+    int64_t* q2_sum;
+    uint64_t* q4_sum;
+    uint32_t* hist;
+    int32_t* e_last;
+    int32_t* m_last;
+    int32_t* d_last;
+    uint64_t* swap_acc;
+    uint32_t* swap_log;
+    int64_t swap_log_rounds; /* capacity of swap_log (in) */
+    int64_t swap_rounds;     /* exchange rounds done (out) */
+    int64_t n_meas;          /* measurements done (out) */
+    uint64_t boundary;       /* exchange decisions within 2^-40 (relative) of
+                                their acceptance probability (out; must be 0) */
+} csg_observables;
+
+/* Device-side accumulators for csg_pt_run_device (device pointers, any may be
+ * NULL).  swap_log row k holds global exchange round swap_round0 + k. */
+typedef struct csg_device_obs {
+    int64_t* e_sum;
+    int64_t* m_sum;
+    int64_t* q_sum;
+    int64_t* q2_sum;
+    uint64_t* q4_sum;
+    uint32_t* hist;
+    int32_t* e_last;
+    int32_t* m_last;
+    int32_t* d_last;
+    uint64_t* swap_acc;
+    uint32_t* swap_log;
+    int64_t swap_log_rounds;
+    int64_t swap_round0;
+    uint64_t* boundary;
+} csg_device_obs;
+
+/* Launch plan: quads per CTA, CTAs per sample word (cluster size), threads
+ * per quad, dynamic shared memory bytes. */
+typedef struct csg_plan {
+    int32_t quads_per_cta;
+    int32_t ctas_per_word;
+    int32_t threads_per_quad;
+    int32_t smem_bytes;
+} csg_plan;
+
+typedef struct csg_engine csg_engine;
+
+/* Message of the last failure on this thread ("" if none). */
+const char* csg_last_error(void);
+
+/* eamsim::eamsim (eamsim.cu:516-543): validate the configuration, allocate
+ * device state on the current CUDA device. */
+int csg_engine_create(const csg_config* cfg, csg_engine** out);
+
+/* eamsim::~eamsim (eamsim.cu:546-559). NULL is accepted. */
+int csg_engine_destroy(csg_engine* e);
+
+/* eamsim::init_lattice (eamsim.cu:622-652): +-J bonds and uniform random
+ * spins from the seed, generated on the device.  Resets the sweep counter
+ * and the observables. */
+int csg_init_lattice(csg_engine* e);
+
+/* Host <-> device state in the canonical layout (counts in uint32 words:
+ * spins W*C*T*N, bonds W*3*N).  set_state resets observables and sets the
+ * sweep counter to `sweep`. */
+int csg_set_state(csg_engine* e, const uint32_t* spins, size_t n_spins, const uint32_t* bonds,
+                  size_t n_bonds, int64_t sweep);
+int csg_get_state(csg_engine* e, uint32_t* spins, size_t n_spins, uint32_t* bonds,
+                  size_t n_bonds, int64_t* sweep);
+
+/* run_simulation_section (eamsim.cu:347-416) looped as in
+ * eamsim::run_simulation (eamsim.cu:689-709): n_sweeps Metropolis sweeps
+ * with the exchange and measurement schedule of the configuration,
+ * continuing from the engine's sweep counter.  Asynchronous on the engine's
+ * stream; csg_get_observables / csg_get_state synchronise. */
+int csg_run(csg_engine* e, int64_t n_sweeps);
+
+/* Copy the accumulated observables to host arrays. */
+int csg_get_observables(csg_engine* e, csg_observables* out);
+
+/* Reset all accumulators to zero. */
+int csg_reset_observables(csg_engine* e);
+
+/* rearrange + compute_q (eamsim.cu:419-511) and the e/m output of
+ * eamsim.cu:407-415: observable records obs_s (eamsim.cuh:55-62) of the
+ * current state, 11 floats {e[2], m[2], q_0, q_1_r[3], q_1_i[3]} per
+ * (sample, temperature), shape [32W][T][11].  Requires n_copies == 2. */
+int csg_obs_records(csg_engine* e, float* rec, size_t n_floats);
+
+/* eamsim::save_checkpoint / load_checkpoint (eamsim.cu:655-676): the
+ * reference's checkpoint layout uint32 [2*32W][N] — lattice 2*sample+copy,
+ * site (z*L+y)*L+x, bits 0..T-1 spins by temperature, bits 26..31 the six
+ * bonds (-x,+x,-y,+y,-z,+z; bit 1 = ferromagnetic).  Requires
+ * n_copies == 2 and n_temps <= 24.  load_checkpoint checks that the bond
+ * bits agree between the ends of every bond and between the two copies. */
+int csg_save_checkpoint(csg_engine* e, uint32_t* ref, size_t n_words);
+int csg_load_checkpoint(csg_engine* e, const uint32_t* ref, size_t n_words, int64_t sweep);
+
+/* run_simulation_section (eamsim.cu:347-416) on caller-owned device buffers:
+ * n_sweeps sweeps of `spins` (canonical layout, device memory) starting at
+ * global sweep index sweep0, adding to the device accumulators of `obs`
+ * (may be NULL).  stream: a cudaStream_t (NULL = legacy default stream). */
+int csg_pt_run_device(const csg_config* cfg, uint32_t* spins, const uint32_t* bonds,
+                      const csg_device_obs* obs, int64_t sweep0, int64_t n_sweeps, void* stream);
+
+/* init_multispins + init_coupling_constants (eamsim.cu:562-619) into
+ * caller-owned device buffers, from the seed. */
+int csg_init_device(const csg_config* cfg, uint32_t* spins, uint32_t* bonds, void* stream);
+
+/* Launch plan the engine picks for a configuration (no counterpart in the
+ * reference, whose launch shape is fixed at eamsim.cu:695). */
+int csg_query_plan(const csg_config* cfg, csg_plan* out);
+
+/* Force quads_per_cta for later launches (must divide n_copies*n_temps/4);
+ * NULL or quads_per_cta == 0 restores the automatic plan. */
+int csg_set_plan_override(const csg_plan* plan);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CSG_H */

@@ -1,0 +1,60 @@
+"""Build libcsg.so (sm_100a) and the csg command-line driver in-tree.
+
+Usage: python spin-glass_b200/build.py [--force]
+"""
+from __future__ import annotations
+
+import os
+import pathlib
+import subprocess
+import sys
+
+PKG = pathlib.Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+LIB = PKG / "libcsg.so"
+CLI = PKG / "csg"
+
+NVCC = os.environ.get("NVCC", "nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
+          "-ffp-contract=off", "-fmad=false", f"-I{ROOT / 'include'}", f"-I{CSRC}"]
+
+LIB_SOURCES = [CSRC / "csg_engine.cu"]
+LIB_DEPS = LIB_SOURCES + sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "csg.h"]
+CLI_SOURCES = [CSRC / "csg_main.cpp"]
+
+
+def _stale(target: pathlib.Path, deps) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(d.exists() and d.stat().st_mtime > t for d in deps)
+
+
+def build_lib(force: bool = False) -> pathlib.Path:
+    if force or _stale(LIB, LIB_DEPS):
+        cmd = [NVCC, *ARCH, *COMMON, "-shared", "-o", str(LIB), *map(str, LIB_SOURCES)]
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+def build_cli(force: bool = False) -> pathlib.Path | None:
+    if not all(s.exists() for s in CLI_SOURCES):
+        return None
+    deps = CLI_SOURCES + [LIB, ROOT / "include" / "csg.h"]
+    if force or _stale(CLI, deps):
+        cmd = ["g++", "-O2", "-std=c++17", f"-I{ROOT / 'include'}", "-o", str(CLI),
+               *map(str, CLI_SOURCES), f"-L{PKG}", "-lcsg", "-Wl,-rpath,$ORIGIN"]
+        subprocess.run(cmd, check=True)
+    return CLI
+
+
+def build(force: bool = False) -> None:
+    build_lib(force)
+    build_cli(force)
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv)
+    print(LIB)

@@ -1,0 +1,751 @@
+// csg_engine.cu — host side of libcsg.so: configuration checks, acceptance
+// tables, launch planning and the C ABI declared in include/csg.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "csg.h"
+#include "philox.cuh"
+#include "pt_kernel.cuh"
+#include "aux_kernels.cuh"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define CSG_CUDA(call)                                                                    \
+    do {                                                                                  \
+        const cudaError_t e_ = (call);                                                    \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(CSG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+bool lattice_supported(int L) { return L >= 4 && L <= 24 && L % 2 == 0; }
+
+int validate(const csg_config* cfg) {
+    if (!cfg) return fail(CSG_ERR_ARG, "null configuration");
+    const csg_dims& d = cfg->dims;
+    if (d.L < 4 || d.L % 2 != 0) return fail(CSG_ERR_ARG, "L must be even and >= 4");
+    if (!lattice_supported(d.L))
+        return fail(CSG_ERR_UNSUPPORTED, "L=" + std::to_string(d.L) + " outside 4..24");
+    if (d.n_words < 1) return fail(CSG_ERR_ARG, "n_words must be >= 1");
+    if (d.n_copies != 1 && d.n_copies != 2) return fail(CSG_ERR_ARG, "n_copies must be 1 or 2");
+    if (d.n_temps < 4 || d.n_temps > csg::kMaxT || d.n_temps % 4 != 0)
+        return fail(CSG_ERR_ARG, "n_temps must be a multiple of 4 in 4..64");
+    if (!(cfg->H >= 0.0 && cfg->H <= 4.0)) return fail(CSG_ERR_ARG, "H out of range");
+    if (!cfg->betas) return fail(CSG_ERR_ARG, "null betas");
+    for (int t = 0; t < d.n_temps; ++t)
+        if (!(cfg->betas[t] >= 0.0) || !std::isfinite(cfg->betas[t]))
+            return fail(CSG_ERR_ARG, "betas must be finite and >= 0");
+    if (cfg->sched.sweeps_per_swap < 0 || cfg->sched.sweeps_per_meas < 0 ||
+        cfg->sched.meas_start < 0)
+        return fail(CSG_ERR_ARG, "negative schedule entry");
+    if (cfg->swap_log_rounds < 0) return fail(CSG_ERR_ARG, "negative swap_log_rounds");
+    return CSG_OK;
+}
+
+// Acceptance table: for centre spin bit s and U unsatisfied bonds the energy
+// change of a flip is dE = 12 - 4U + 2H(2s-1); the flip is accepted when a
+// 32-bit draw r satisfies r < floor(exp(-beta dE) 2^32), and always when
+// that value reaches 2^32 (dE <= 0).  ucut[t][s] is the first such U.
+// Returns whether the H=0 kernel (3 thresholds, U >= 3 always) describes the
+// table exactly.
+bool build_tables(const csg_config& cfg, csg::PtTables& tab) {
+    std::memset(&tab, 0, sizeof(tab));
+    bool h0_exact = true;
+    for (int t = 0; t < cfg.dims.n_temps; ++t) {
+        tab.beta[t] = cfg.betas[t];
+        for (int s = 0; s < 2; ++s) {
+            int cut = 7;
+            for (int U = 0; U <= 6; ++U) {
+                const double dE = 12.0 - 4.0 * U + 2.0 * cfg.H * (s ? 1.0 : -1.0);
+                uint64_t v = (uint64_t)1 << 32;
+                if (dE > 0.0) v = (uint64_t)(std::exp(-cfg.betas[t] * dE) * 4294967296.0);
+                if (v >= ((uint64_t)1 << 32)) {
+                    if (cut == 7) cut = U;
+                    tab.thr[t][s][U] = 0xFFFFFFFFu;
+                } else {
+                    if (cut != 7) h0_exact = false;  // non-monotone (cannot happen for beta >= 0)
+                    tab.thr[t][s][U] = (uint32_t)v;
+                }
+            }
+            tab.ucut[t][s] = (uint8_t)cut;
+            if (cut != 3) h0_exact = false;
+        }
+        for (int U = 0; U < 3; ++U)
+            if (tab.thr[t][0][U] != tab.thr[t][1][U]) h0_exact = false;
+    }
+    return h0_exact && cfg.H == 0.0;
+}
+
+using KernelFn = void (*)(csg::PtParams);
+
+template <int L>
+KernelFn kernel_for(bool gen) {
+    return gen ? csg::pt_resident_kernel<L, true> : csg::pt_resident_kernel<L, false>;
+}
+
+KernelFn select_kernel(int L, bool gen) {
+    switch (L) {
+        case 4: return kernel_for<4>(gen);
+        case 6: return kernel_for<6>(gen);
+        case 8: return kernel_for<8>(gen);
+        case 10: return kernel_for<10>(gen);
+        case 12: return kernel_for<12>(gen);
+        case 14: return kernel_for<14>(gen);
+        case 16: return kernel_for<16>(gen);
+        case 18: return kernel_for<18>(gen);
+        case 20: return kernel_for<20>(gen);
+        case 22: return kernel_for<22>(gen);
+        case 24: return kernel_for<24>(gen);
+        default: return nullptr;
+    }
+}
+
+size_t smem_for(int L, int Qc) {
+    switch (L) {
+        case 4: return csg::SmemMap<4>::bytes(Qc);
+        case 6: return csg::SmemMap<6>::bytes(Qc);
+        case 8: return csg::SmemMap<8>::bytes(Qc);
+        case 10: return csg::SmemMap<10>::bytes(Qc);
+        case 12: return csg::SmemMap<12>::bytes(Qc);
+        case 14: return csg::SmemMap<14>::bytes(Qc);
+        case 16: return csg::SmemMap<16>::bytes(Qc);
+        case 18: return csg::SmemMap<18>::bytes(Qc);
+        case 20: return csg::SmemMap<20>::bytes(Qc);
+        case 22: return csg::SmemMap<22>::bytes(Qc);
+        case 24: return csg::SmemMap<24>::bytes(Qc);
+        default: return 0;
+    }
+}
+
+constexpr size_t kMaxSmem = 227 * 1024;
+
+struct Plan {
+    int Qc = 0, K = 0, TPQ = 0;
+    size_t smem = 0;
+};
+
+std::mutex g_plan_mu;
+csg_plan g_override = {0, 0, 0, 0};
+
+int prepare_kernel(KernelFn fn, size_t smem, int K) {
+    CSG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (K > 8) CSG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    return CSG_OK;
+}
+
+void fill_launch(cudaLaunchConfig_t& lc, cudaLaunchAttribute* attr, int W, const Plan& pl,
+                 cudaStream_t st) {
+    lc = cudaLaunchConfig_t{};
+    lc.gridDim = dim3((unsigned)(W * pl.K), 1, 1);
+    lc.blockDim = dim3((unsigned)(pl.Qc * pl.TPQ), 1, 1);
+    lc.dynamicSmemBytes = pl.smem;
+    lc.stream = st;
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)pl.K;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    lc.attrs = attr;
+    lc.numAttrs = 1;
+}
+
+// Launch plan: split the G = C*T/4 quads of a word over K = G/Qc CTAs of a
+// cluster.  The score is the number of quads the busiest SM must sweep
+// (waves of co-resident clusters times the quads per SM in a wave); ties go
+// to the smaller cluster (fewer cross-CTA exchanges).
+int make_plan(const csg_config& cfg, bool gen, Plan& out) {
+    const int L = cfg.dims.L, W = cfg.dims.n_words;
+    const int G = cfg.dims.n_copies * cfg.dims.n_temps / 4;
+    const int tpq = csg::tpq_for(L);
+    KernelFn fn = select_kernel(L, gen);
+    if (!fn) return fail(CSG_ERR_UNSUPPORTED, "no kernel for L");
+    {
+        std::lock_guard<std::mutex> lk(g_plan_mu);
+        if (g_override.quads_per_cta > 0) {
+            const int Qc = g_override.quads_per_cta;
+            if (G % Qc != 0) return fail(CSG_ERR_ARG, "plan override does not divide the quads");
+            out.Qc = Qc;
+            out.K = G / Qc;
+            out.TPQ = tpq;
+            out.smem = smem_for(L, Qc);
+            if (out.K > 16 || out.smem > kMaxSmem || Qc * tpq > csg::kMaxThreads)
+                return fail(CSG_ERR_UNSUPPORTED, "plan override exceeds device limits");
+            return prepare_kernel(fn, out.smem, out.K);
+        }
+    }
+    int dev = 0, nsm = 0;
+    CSG_CUDA(cudaGetDevice(&dev));
+    CSG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    long best = -1;
+    for (int Qc = 1; Qc <= G; ++Qc) {
+        if (G % Qc) continue;
+        Plan pl;
+        pl.Qc = Qc;
+        pl.K = G / Qc;
+        pl.TPQ = tpq;
+        pl.smem = smem_for(L, Qc);
+        if (pl.K > 16 || pl.smem > kMaxSmem || Qc * tpq > csg::kMaxThreads) continue;
+        if (prepare_kernel(fn, pl.smem, pl.K) != CSG_OK) continue;
+        cudaLaunchConfig_t lc;
+        cudaLaunchAttribute attr[1];
+        fill_launch(lc, attr, W, pl, nullptr);
+        int nclusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&nclusters, fn, &lc) != cudaSuccess || nclusters < 1) {
+            cudaGetLastError();
+            continue;
+        }
+        const long waves = (W + nclusters - 1) / nclusters;
+        const long per_wave = (long)std::min(W, nclusters) * pl.K;
+        const long load = waves * ((per_wave + nsm - 1) / nsm) * Qc;
+        const long score = load * 64 + pl.K;
+        if (best < 0 || score < best) {
+            best = score;
+            out = pl;
+        }
+    }
+    if (best < 0) return fail(CSG_ERR_UNSUPPORTED, "no launch plan fits this configuration");
+    return prepare_kernel(fn, out.smem, out.K);
+}
+
+int64_t count_events(int64_t s0, int64_t n, int64_t k, int64_t first_sweep) {
+    // number of s in [max(s0, first_sweep), s0+n) with (s+1) % k == 0
+    if (k <= 0 || n <= 0) return 0;
+    const int64_t lo = std::max(s0, first_sweep) + 1, hi = s0 + n;
+    if (hi < lo) return 0;
+    return hi / k - (lo - 1) / k;
+}
+
+int fill_params(const csg_config& cfg, csg::PtParams& P, bool& gen) {
+    std::memset(&P, 0, sizeof(P));
+    gen = !build_tables(cfg, P.tab);
+    P.H = cfg.H;
+    P.k0 = (uint32_t)cfg.seed;
+    P.k1 = (uint32_t)(cfg.seed >> 32);
+    P.W = cfg.dims.n_words;
+    P.C = cfg.dims.n_copies;
+    P.T = cfg.dims.n_temps;
+    P.Q = cfg.dims.n_temps / 4;
+    P.sps = cfg.sched.sweeps_per_swap;
+    P.spm = cfg.sched.sweeps_per_meas;
+    P.meas_start = cfg.sched.meas_start;
+    P.flags = (cfg.flags & CSG_MEASURE_M) ? csg::kFlagMeasureM : 0;
+    return CSG_OK;
+}
+
+constexpr int64_t kSweepsPerLaunch = 1024;
+
+int run_device(const csg_config& cfg, uint32_t* spins, const uint32_t* bonds,
+               const csg_device_obs* obs, int64_t sweep0, int64_t n_sweeps, cudaStream_t st) {
+    csg::PtParams P;
+    bool gen = false;
+    fill_params(cfg, P, gen);
+    Plan pl;
+    if (int rc = make_plan(cfg, gen, pl)) return rc;
+    KernelFn fn = select_kernel(cfg.dims.L, gen);
+    P.spins = spins;
+    P.bonds = bonds;
+    if (obs) {
+        P.e_sum = reinterpret_cast<long long*>(obs->e_sum);
+        P.m_sum = reinterpret_cast<long long*>(obs->m_sum);
+        P.q_sum = reinterpret_cast<long long*>(obs->q_sum);
+        P.q2_sum = reinterpret_cast<long long*>(obs->q2_sum);
+        P.q4_sum = reinterpret_cast<unsigned long long*>(obs->q4_sum);
+        P.hist = obs->hist;
+        P.e_last = obs->e_last;
+        P.m_last = obs->m_last;
+        P.d_last = obs->d_last;
+        P.swap_acc = reinterpret_cast<unsigned long long*>(obs->swap_acc);
+        P.swap_log = obs->swap_log;
+        P.swap_log_rounds = obs->swap_log_rounds;
+        P.swap_round0 = obs->swap_round0;
+        P.boundary = reinterpret_cast<unsigned long long*>(obs->boundary);
+    }
+    P.K = pl.K;
+    P.Qc = pl.Qc;
+    for (int64_t done = 0; done < n_sweeps; done += kSweepsPerLaunch) {
+        P.sweep0 = sweep0 + done;
+        P.n_sweeps = (int)std::min<int64_t>(kSweepsPerLaunch, n_sweeps - done);
+        cudaLaunchConfig_t lc;
+        cudaLaunchAttribute attr[1];
+        fill_launch(lc, attr, cfg.dims.n_words, pl, st);
+        CSG_CUDA(cudaLaunchKernelEx(&lc, fn, P));
+    }
+    return CSG_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Engine object
+// ---------------------------------------------------------------------------
+struct csg_engine {
+    csg_config cfg{};
+    std::vector<double> betas;
+    cudaStream_t stream = nullptr;
+    size_t n_spins = 0, n_bonds = 0, n_e = 0, n_q = 0, n_hist = 0;
+    uint32_t* spins = nullptr;
+    uint32_t* bonds = nullptr;
+    // device accumulators
+    int64_t *e_sum = nullptr, *m_sum = nullptr, *q_sum = nullptr, *q2_sum = nullptr;
+    uint64_t* q4_sum = nullptr;
+    uint32_t* hist = nullptr;
+    int32_t *e_last = nullptr, *m_last = nullptr, *d_last = nullptr;
+    uint64_t* swap_acc = nullptr;
+    uint32_t* swap_log = nullptr;
+    uint64_t* boundary = nullptr;
+    int64_t sweep = 0, n_meas = 0, swap_rounds = 0, swap_round0 = 0;
+};
+
+namespace {
+
+template <typename T>
+int dalloc(T** p, size_t n) {
+    if (n == 0) {
+        *p = nullptr;
+        return CSG_OK;
+    }
+    const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return fail(CSG_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    return CSG_OK;
+}
+
+void free_engine(csg_engine* e) {
+    void* ptrs[] = {e->spins, e->bonds, e->e_sum, e->m_sum, e->q_sum, e->q2_sum, e->q4_sum,
+                    e->hist, e->e_last, e->m_last, e->d_last, e->swap_acc, e->swap_log,
+                    e->boundary};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (e->stream) cudaStreamDestroy(e->stream);
+}
+
+int reset_obs(csg_engine* e) {
+    struct Z {
+        void* p;
+        size_t bytes;
+    } z[] = {{e->e_sum, e->n_e * 8}, {e->m_sum, e->n_e * 8}, {e->q_sum, e->n_q * 8},
+             {e->q2_sum, e->n_q * 8}, {e->q4_sum, e->n_q * 16}, {e->hist, e->n_hist * 4},
+             {e->e_last, e->n_e * 4}, {e->m_last, e->n_e * 4}, {e->d_last, e->n_q * 4},
+             {e->swap_acc, (size_t)e->cfg.dims.n_copies * e->cfg.dims.n_temps * 8},
+             {e->swap_log, (size_t)e->cfg.swap_log_rounds * e->n_e / 32 * 4},
+             {e->boundary, 8}};
+    for (auto& zz : z)
+        if (zz.p && zz.bytes) CSG_CUDA(cudaMemsetAsync(zz.p, 0, zz.bytes, e->stream));
+    e->n_meas = 0;
+    e->swap_rounds = 0;
+    const int64_t k = e->cfg.sched.sweeps_per_swap;
+    e->swap_round0 = k > 0 ? (e->sweep + k) / k - 1 : 0;
+    return CSG_OK;
+}
+
+csg_device_obs device_obs(const csg_engine* e) {
+    csg_device_obs o{};
+    o.e_sum = e->e_sum;
+    o.m_sum = e->m_sum;
+    o.q_sum = e->q_sum;
+    o.q2_sum = e->q2_sum;
+    o.q4_sum = e->q4_sum;
+    o.hist = e->hist;
+    o.e_last = e->e_last;
+    o.m_last = e->m_last;
+    o.d_last = e->d_last;
+    o.swap_acc = e->swap_acc;
+    o.swap_log = e->swap_log;
+    o.swap_log_rounds = e->cfg.swap_log_rounds;
+    o.swap_round0 = e->swap_round0;
+    o.boundary = e->boundary;
+    return o;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* csg_last_error(void) { return g_err.c_str(); }
+
+int csg_engine_create(const csg_config* cfg, csg_engine** out) {
+    if (!out) return fail(CSG_ERR_ARG, "null output pointer");
+    *out = nullptr;
+    if (int rc = validate(cfg)) return rc;
+    csg_engine* e = new (std::nothrow) csg_engine();
+    if (!e) return fail(CSG_ERR_NOMEM, "host allocation failed");
+    e->cfg = *cfg;
+    e->betas.assign(cfg->betas, cfg->betas + cfg->dims.n_temps);
+    e->cfg.betas = e->betas.data();
+    const csg_dims& d = cfg->dims;
+    const size_t N = (size_t)d.L * d.L * d.L;
+    e->n_spins = (size_t)d.n_words * d.n_copies * d.n_temps * N;
+    e->n_bonds = (size_t)d.n_words * 3 * N;
+    e->n_e = (size_t)d.n_words * d.n_copies * d.n_temps * 32;
+    e->n_q = d.n_copies == 2 ? (size_t)d.n_words * d.n_temps * 32 : 0;
+    e->n_hist = d.n_copies == 2 ? (size_t)d.n_temps * (N + 1) : 0;
+    int rc = CSG_OK;
+    auto chk = [&](int r) {
+        if (rc == CSG_OK) rc = r;
+    };
+    if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        e->stream = nullptr;
+        delete e;
+        return fail(CSG_ERR_CUDA, "cudaStreamCreate failed");
+    }
+    chk(dalloc(&e->spins, e->n_spins));
+    chk(dalloc(&e->bonds, e->n_bonds));
+    chk(dalloc(&e->e_sum, e->n_e));
+    chk(dalloc(&e->m_sum, e->n_e));
+    chk(dalloc(&e->e_last, e->n_e));
+    chk(dalloc(&e->m_last, e->n_e));
+    chk(dalloc(&e->q_sum, e->n_q));
+    chk(dalloc(&e->q2_sum, e->n_q));
+    chk(dalloc(&e->q4_sum, 2 * e->n_q));
+    chk(dalloc(&e->d_last, e->n_q));
+    chk(dalloc(&e->hist, e->n_hist));
+    chk(dalloc(&e->swap_acc, (size_t)d.n_copies * d.n_temps));
+    chk(dalloc(&e->swap_log, (size_t)cfg->swap_log_rounds * e->n_e / 32));
+    chk(dalloc(&e->boundary, 1));
+    if (rc == CSG_OK) rc = reset_obs(e);
+    if (rc == CSG_OK) {
+        // A launch plan must exist before the engine is handed out.
+        csg::PtParams P;
+        bool gen = false;
+        fill_params(e->cfg, P, gen);
+        Plan pl;
+        rc = make_plan(e->cfg, gen, pl);
+    }
+    if (rc != CSG_OK) {
+        const std::string msg = g_err;
+        free_engine(e);
+        delete e;
+        g_err = msg;
+        return rc;
+    }
+    *out = e;
+    return CSG_OK;
+}
+
+int csg_engine_destroy(csg_engine* e) {
+    if (!e) return CSG_OK;
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    free_engine(e);
+    delete e;
+    return CSG_OK;
+}
+
+int csg_init_device(const csg_config* cfg, uint32_t* spins, uint32_t* bonds, void* stream) {
+    if (int rc = validate(cfg)) return rc;
+    if (!spins || !bonds) return fail(CSG_ERR_ARG, "null device buffer");
+    const csg_dims& d = cfg->dims;
+    const long N = (long)d.L * d.L * d.L;
+    const long total = (long)d.n_words * N;
+    const int block = 256;
+    csg::init_kernel<<<(unsigned)((total + block - 1) / block), block, 0, (cudaStream_t)stream>>>(
+        spins, bonds, d.L, d.n_words, d.n_copies, d.n_temps / 4, (uint32_t)cfg->seed,
+        (uint32_t)(cfg->seed >> 32));
+    CSG_CUDA(cudaGetLastError());
+    return CSG_OK;
+}
+
+int csg_init_lattice(csg_engine* e) {
+    if (!e) return fail(CSG_ERR_ARG, "null engine");
+    if (int rc = csg_init_device(&e->cfg, e->spins, e->bonds, e->stream)) return rc;
+    e->sweep = 0;
+    return reset_obs(e);
+}
+
+int csg_set_state(csg_engine* e, const uint32_t* spins, size_t n_spins, const uint32_t* bonds,
+                  size_t n_bonds, int64_t sweep) {
+    if (!e) return fail(CSG_ERR_ARG, "null engine");
+    if (!spins || n_spins != e->n_spins) return fail(CSG_ERR_ARG, "spins size mismatch");
+    if (!bonds || n_bonds != e->n_bonds) return fail(CSG_ERR_ARG, "bonds size mismatch");
+    if (sweep < 0) return fail(CSG_ERR_ARG, "negative sweep index");
+    CSG_CUDA(cudaMemcpyAsync(e->spins, spins, n_spins * 4, cudaMemcpyHostToDevice, e->stream));
+    CSG_CUDA(cudaMemcpyAsync(e->bonds, bonds, n_bonds * 4, cudaMemcpyHostToDevice, e->stream));
+    e->sweep = sweep;
+    return reset_obs(e);
+}
+
+int csg_get_state(csg_engine* e, uint32_t* spins, size_t n_spins, uint32_t* bonds,
+                  size_t n_bonds, int64_t* sweep) {
+    if (!e) return fail(CSG_ERR_ARG, "null engine");
+    if (spins) {
+        if (n_spins != e->n_spins) return fail(CSG_ERR_ARG, "spins size mismatch");
+        CSG_CUDA(cudaMemcpyAsync(spins, e->spins, n_spins * 4, cudaMemcpyDeviceToHost, e->stream));
+    }
+    if (bonds) {
+        if (n_bonds != e->n_bonds) return fail(CSG_ERR_ARG, "bonds size mismatch");
+        CSG_CUDA(cudaMemcpyAsync(bonds, e->bonds, n_bonds * 4, cudaMemcpyDeviceToHost, e->stream));
+    }
+    CSG_CUDA(cudaStreamSynchronize(e->stream));
+    if (sweep) *sweep = e->sweep;
+    return CSG_OK;
+}
+
+int csg_run(csg_engine* e, int64_t n_sweeps) {
+    if (!e) return fail(CSG_ERR_ARG, "null engine");
+    if (n_sweeps < 0) return fail(CSG_ERR_ARG, "negative sweep count");
+    if (n_sweeps == 0) return CSG_OK;
+    const csg_device_obs o = device_obs(e);
+    if (int rc = run_device(e->cfg, e->spins, e->bonds, &o, e->sweep, n_sweeps, e->stream))
+        return rc;
+    const csg_schedule& sc = e->cfg.sched;
+    e->swap_rounds += count_events(e->sweep, n_sweeps, sc.sweeps_per_swap, 0);
+    e->n_meas += count_events(e->sweep, n_sweeps, sc.sweeps_per_meas, sc.meas_start);
+    e->sweep += n_sweeps;
+    return CSG_OK;
+}
+
+int csg_reset_observables(csg_engine* e) {
+    if (!e) return fail(CSG_ERR_ARG, "null engine");
+    return reset_obs(e);
+}
+
+int csg_get_observables(csg_engine* e, csg_observables* out) {
+    if (!e || !out) return fail(CSG_ERR_ARG, "null argument");
+    struct C {
+        void* dst;
+        const void* src;
+        size_t bytes;
+    } cp[] = {{out->e_sum, e->e_sum, e->n_e * 8},   {out->m_sum, e->m_sum, e->n_e * 8},
+              {out->q_sum, e->q_sum, e->n_q * 8},   {out->q2_sum, e->q2_sum, e->n_q * 8},
+              {out->q4_sum, e->q4_sum, e->n_q * 16}, {out->hist, e->hist, e->n_hist * 4},
+              {out->e_last, e->e_last, e->n_e * 4}, {out->m_last, e->m_last, e->n_e * 4},
+              {out->d_last, e->d_last, e->n_q * 4},
+              {out->swap_acc, e->swap_acc, (size_t)e->cfg.dims.n_copies * e->cfg.dims.n_temps * 8}};
+    for (auto& c : cp)
+        if (c.dst && c.src && c.bytes)
+            CSG_CUDA(cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, e->stream));
+    if (out->swap_log && e->swap_log) {
+        const int64_t rows = std::min<int64_t>(out->swap_log_rounds, e->cfg.swap_log_rounds);
+        if (rows > 0)
+            CSG_CUDA(cudaMemcpyAsync(out->swap_log, e->swap_log, (size_t)rows * e->n_e / 32 * 4,
+                                     cudaMemcpyDeviceToHost, e->stream));
+    }
+    uint64_t b = 0;
+    CSG_CUDA(cudaMemcpyAsync(&b, e->boundary, 8, cudaMemcpyDeviceToHost, e->stream));
+    CSG_CUDA(cudaStreamSynchronize(e->stream));
+    out->boundary = b;
+    out->n_meas = e->n_meas;
+    out->swap_rounds = e->swap_rounds;
+    return CSG_OK;
+}
+
+int csg_pt_run_device(const csg_config* cfg, uint32_t* spins, const uint32_t* bonds,
+                      const csg_device_obs* obs, int64_t sweep0, int64_t n_sweeps, void* stream) {
+    if (int rc = validate(cfg)) return rc;
+    if (!spins || !bonds) return fail(CSG_ERR_ARG, "null device buffer");
+    if (sweep0 < 0 || n_sweeps < 0) return fail(CSG_ERR_ARG, "negative sweep index or count");
+    if (n_sweeps == 0) return CSG_OK;
+    return run_device(*cfg, spins, bonds, obs, sweep0, n_sweeps, (cudaStream_t)stream);
+}
+
+int csg_query_plan(const csg_config* cfg, csg_plan* out) {
+    if (int rc = validate(cfg)) return rc;
+    if (!out) return fail(CSG_ERR_ARG, "null output");
+    csg::PtParams P;
+    bool gen = false;
+    fill_params(*cfg, P, gen);
+    Plan pl;
+    if (int rc = make_plan(*cfg, gen, pl)) return rc;
+    out->quads_per_cta = pl.Qc;
+    out->ctas_per_word = pl.K;
+    out->threads_per_quad = pl.TPQ;
+    out->smem_bytes = (int32_t)pl.smem;
+    return CSG_OK;
+}
+
+int csg_set_plan_override(const csg_plan* plan) {
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    if (!plan) {
+        g_override = csg_plan{0, 0, 0, 0};
+        return CSG_OK;
+    }
+    if (plan->quads_per_cta < 0) return fail(CSG_ERR_ARG, "negative quads_per_cta");
+    g_override = *plan;
+    return CSG_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Reference-format outputs: observable records and checkpoints
+// ---------------------------------------------------------------------------
+namespace {
+
+size_t slot_of(int L, int x, int y, int z) {
+    const size_t N = (size_t)L * L * L;
+    return (size_t)((x + y + z) & 1) * (N / 2) + (size_t)(z * L + y) * (L / 2) + (size_t)(x >> 1);
+}
+
+size_t spin_at(const csg_dims& d, int w, int c, int t, size_t slot) {
+    const size_t N = (size_t)d.L * d.L * d.L;
+    return ((((size_t)w * d.n_copies + c) * (d.n_temps / 4) + (size_t)(t >> 2)) * N + slot) * 4 +
+           (size_t)(t & 3);
+}
+
+}  // namespace
+
+extern "C" {
+
+// Records follow eamsim.cu:320-325 (e = -(2S-3N + H M)/N, m = M/N, float
+// arithmetic as in the reference) and eamsim.cu:477-509 (q_0 = sum s1 s2 / N,
+// q_1 = sum s1 s2 exp(i k x) / N with k = 2 pi / L), the latter formed from
+// exact per-plane integer sums combined in double precision.
+int csg_obs_records(csg_engine* e, float* rec, size_t n_floats) {
+    if (!e || !rec) return fail(CSG_ERR_ARG, "null argument");
+    const csg_dims& d = e->cfg.dims;
+    if (d.n_copies != 2) return fail(CSG_ERR_UNSUPPORTED, "observable records need two copies");
+    const int L = d.L, W = d.n_words, T = d.n_temps;
+    const size_t need = (size_t)32 * W * T * 11;
+    if (n_floats != need) return fail(CSG_ERR_ARG, "record buffer size mismatch");
+    const size_t nE = (size_t)W * 2 * T * 32, nD = (size_t)W * T * 32, nP = nD * 3 * L;
+    int *de = nullptr, *dm = nullptr, *dd = nullptr, *dp = nullptr;
+    int rc = dalloc(&de, nE);
+    if (!rc) rc = dalloc(&dm, nE);
+    if (!rc) rc = dalloc(&dd, nD);
+    if (!rc) rc = dalloc(&dp, nP);
+    std::vector<int> he(nE), hm(nE), hd(nD), hp(nP);
+    if (!rc) {
+        const int warps = 4;
+        const unsigned blocks = (unsigned)((W * T + warps - 1) / warps);
+        const size_t sh = (size_t)warps * 32 * 3 * L * sizeof(int);
+        csg::measure_kernel<<<blocks, warps * 32, sh, e->stream>>>(e->spins, e->bonds, L, W, T, de,
+                                                                   dm, dd, dp);
+        cudaError_t ce = cudaGetLastError();
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(he.data(), de, nE * 4, cudaMemcpyDeviceToHost, e->stream);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(hm.data(), dm, nE * 4, cudaMemcpyDeviceToHost, e->stream);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(hd.data(), dd, nD * 4, cudaMemcpyDeviceToHost, e->stream);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(hp.data(), dp, nP * 4, cudaMemcpyDeviceToHost, e->stream);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+        if (ce != cudaSuccess) rc = fail(CSG_ERR_CUDA, std::string("measure: ") + cudaGetErrorString(ce));
+    }
+    for (void* p : {(void*)de, (void*)dm, (void*)dd, (void*)dp})
+        if (p) cudaFree(p);
+    if (rc) return rc;
+    const int64_t N = (int64_t)L * L * L;
+    const float H = (float)e->cfg.H;
+    const double k = 2.0 * M_PI / L;
+    for (int w = 0; w < W; ++w)
+        for (int b = 0; b < 32; ++b)
+            for (int t = 0; t < T; ++t) {
+                float* o = rec + (((size_t)(32 * w + b)) * T + t) * 11;
+                for (int c = 0; c < 2; ++c) {
+                    const size_t i = (((size_t)w * 2 + c) * T + t) * 32 + b;
+                    const float es = (float)(-he[i]);
+                    const float ms = (float)hm[i];
+                    o[c] = -(es + H * ms) / (float)N;
+                    o[2 + c] = ms / (float)N;
+                }
+                const size_t i = ((size_t)w * T + t) * 32 + b;
+                o[4] = (float)(N - 2 * (int64_t)hd[i]) / (float)N;
+                for (int dir = 0; dir < 3; ++dir) {
+                    double re = 0.0, im = 0.0;
+                    for (int a = 0; a < L; ++a) {
+                        const int64_t P = (int64_t)L * L - 2 * (int64_t)hp[(i * 3 + dir) * L + a];
+                        re += (double)P * std::cos(k * a);
+                        im += (double)P * std::sin(k * a);
+                    }
+                    o[5 + dir] = (float)(re / (double)N);
+                    o[8 + dir] = (float)(im / (double)N);
+                }
+            }
+    return CSG_OK;
+}
+
+// Reference checkpoint (eamsim.cu:655-676): uint32 [2*32W][N], lattice
+// 2*sample+copy, site (z*L+y)*L+x; bits 0..T-1 spins by temperature, bits
+// 26..31 bonds -x,+x,-y,+y,-z,+z with bit 1 = ferromagnetic (eamsim.cu:598-616).
+int csg_save_checkpoint(csg_engine* e, uint32_t* ref, size_t n_words) {
+    if (!e || !ref) return fail(CSG_ERR_ARG, "null argument");
+    const csg_dims& d = e->cfg.dims;
+    if (d.n_copies != 2 || d.n_temps > 24)
+        return fail(CSG_ERR_UNSUPPORTED, "checkpoint layout needs 2 copies and <= 24 temperatures");
+    const int L = d.L, W = d.n_words, T = d.n_temps;
+    const size_t N = (size_t)L * L * L;
+    if (n_words != (size_t)64 * W * N) return fail(CSG_ERR_ARG, "checkpoint size mismatch");
+    std::vector<uint32_t> sp(e->n_spins), bd(e->n_bonds);
+    if (int rc = csg_get_state(e, sp.data(), sp.size(), bd.data(), bd.size(), nullptr)) return rc;
+    for (int w = 0; w < W; ++w)
+        for (int z = 0; z < L; ++z)
+            for (int y = 0; y < L; ++y)
+                for (int x = 0; x < L; ++x) {
+                    const size_t si = slot_of(L, x, y, z), i = ((size_t)z * L + y) * L + x;
+                    const int xm = (x + L - 1) % L, ym = (y + L - 1) % L, zm = (z + L - 1) % L;
+                    const uint32_t f[6] = {bd[((size_t)w * 3 + 0) * N + slot_of(L, xm, y, z)],
+                                           bd[((size_t)w * 3 + 0) * N + si],
+                                           bd[((size_t)w * 3 + 1) * N + slot_of(L, x, ym, z)],
+                                           bd[((size_t)w * 3 + 1) * N + si],
+                                           bd[((size_t)w * 3 + 2) * N + slot_of(L, x, y, zm)],
+                                           bd[((size_t)w * 3 + 2) * N + si]};
+                    uint32_t sv[2][24];
+                    for (int c = 0; c < 2; ++c)
+                        for (int t = 0; t < T; ++t) sv[c][t] = sp[spin_at(d, w, c, t, si)];
+                    for (int b = 0; b < 32; ++b) {
+                        uint32_t jb = 0;
+                        for (int k = 0; k < 6; ++k) jb |= ((~f[k] >> b) & 1u) << (26 + k);
+                        for (int c = 0; c < 2; ++c) {
+                            uint32_t v = jb;
+                            for (int t = 0; t < T; ++t) v |= ((sv[c][t] >> b) & 1u) << t;
+                            ref[((size_t)2 * (32 * w + b) + c) * N + i] = v;
+                        }
+                    }
+                }
+    return CSG_OK;
+}
+
+int csg_load_checkpoint(csg_engine* e, const uint32_t* ref, size_t n_words, int64_t sweep) {
+    if (!e || !ref) return fail(CSG_ERR_ARG, "null argument");
+    const csg_dims& d = e->cfg.dims;
+    if (d.n_copies != 2 || d.n_temps > 24)
+        return fail(CSG_ERR_UNSUPPORTED, "checkpoint layout needs 2 copies and <= 24 temperatures");
+    const int L = d.L, W = d.n_words, T = d.n_temps;
+    const size_t N = (size_t)L * L * L;
+    if (n_words != (size_t)64 * W * N) return fail(CSG_ERR_ARG, "checkpoint size mismatch");
+    std::vector<uint32_t> sp(e->n_spins, 0u), bd(e->n_bonds, 0u);
+    for (int w = 0; w < W; ++w)
+        for (int z = 0; z < L; ++z)
+            for (int y = 0; y < L; ++y)
+                for (int x = 0; x < L; ++x) {
+                    const size_t si = slot_of(L, x, y, z), i = ((size_t)z * L + y) * L + x;
+                    const size_t nbi[3] = {((size_t)z * L + y) * L + (x + 1) % L,
+                                           ((size_t)z * L + (y + 1) % L) * L + x,
+                                           ((size_t)((z + 1) % L) * L + y) * L + x};
+                    uint32_t f[3] = {0, 0, 0};
+                    uint32_t sv[2][24] = {};
+                    for (int b = 0; b < 32; ++b) {
+                        const uint32_t v0 = ref[((size_t)2 * (32 * w + b)) * N + i];
+                        const uint32_t v1 = ref[((size_t)2 * (32 * w + b) + 1) * N + i];
+                        if ((v0 >> 26) != (v1 >> 26))
+                            return fail(CSG_ERR_STATE, "copies of a sample disagree on its bonds");
+                        for (int k = 0; k < 3; ++k) {
+                            const uint32_t vn = ref[((size_t)2 * (32 * w + b)) * N + nbi[k]];
+                            if (((v0 >> (27 + 2 * k)) & 1u) != ((vn >> (26 + 2 * k)) & 1u))
+                                return fail(CSG_ERR_STATE, "the two ends of a bond disagree");
+                            f[k] |= ((~v0 >> (27 + 2 * k)) & 1u) << b;
+                        }
+                        for (int t = 0; t < T; ++t) {
+                            sv[0][t] |= ((v0 >> t) & 1u) << b;
+                            sv[1][t] |= ((v1 >> t) & 1u) << b;
+                        }
+                    }
+                    for (int k = 0; k < 3; ++k) bd[((size_t)w * 3 + k) * N + si] = f[k];
+                    for (int c = 0; c < 2; ++c)
+                        for (int t = 0; t < T; ++t) sp[spin_at(d, w, c, t, si)] = sv[c][t];
+                }
+    return csg_set_state(e, sp.data(), sp.size(), bd.data(), bd.size(), sweep);
+}
+
+}  // extern "C"
