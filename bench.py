@@ -1,0 +1,340 @@
+"""Benchmark: spin-flip attempts/ns of the parallel-tempering engine on B200.
+
+Workload (the plain engine at production size): L=16 periodic +-J lattice,
+1024 disorder samples (32 uint32 words x 32 bits), 2 copies, 24 temperatures
+geometric in T in [0.2, 2.0], a replica-exchange attempt every sweep, e and q
+measured every sweep (the measurement half of a 65536-sweep run).  One step is
+one section of 1024 sweeps = one kernel launch.  Synthetic, seeded disorder.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  With torchrun, every rank runs its own
+independent set of 1024 samples (weak scaling, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import importlib.util
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+L, W, NCOPY, T = 16, 32, 2, 24
+T_MIN, T_MAX = 0.2, 2.0
+SWEEPS_PER_STEP = 1024
+SWEEP0 = 32768  # timed sections sit in the measurement half of a 65536-sweep run
+SEED = 0x5EED0001
+# Algorithmic integer operations per 32-sample word update (19 logic + 25 Philox
+# share + 3 compares), i.e. 47/32 = 1.47 per spin-flip attempt.
+OPS_PER_WORD_UPDATE = 47
+METRIC = "spin-flip attempts/ns"
+
+
+def _package():
+    pkg_dir = ROOT / "spin-glass_b200"
+    spec = importlib.util.spec_from_file_location(
+        "spin_glass_b200", pkg_dir / "__init__.py", submodule_search_locations=[str(pkg_dir)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["spin_glass_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def attempts_per_sweep() -> int:
+    return L ** 3 * W * 32 * NCOPY * T
+
+
+def workload_config(n_gpus: int) -> dict:
+    return {"workload": "plain PT engine, production size", "L": L, "samples": 32 * W,
+            "copies": NCOPY, "temperatures": T, "T_range": [T_MIN, T_MAX],
+            "sweeps_per_step": SWEEPS_PER_STEP, "swap_every": 1, "measure_every": 1,
+            "field_H": 0.0, "l2": "flushed between timed steps (256 MiB write)",
+            "parallelism": f"sample shards x{n_gpus}"}
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during timing."""
+
+    QUERY = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (getattr(self, "out", "") or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx.append(float(f[1]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[3:7]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def int_peak_ops() -> dict:
+    """Measured LOP3 issue rate of the whole GPU (ops/s)."""
+    lib = C.CDLL(str(ROOT / "spin-glass_b200" / "libcsg_peak.so"))
+    lib.csg_int_peak.argtypes = [C.POINTER(C.c_double), C.c_int]
+    lib.csg_int_peak.restype = C.c_int
+    v = C.c_double()
+    if lib.csg_int_peak(C.byref(v), 5) != 0:
+        raise RuntimeError("integer peak microbenchmark failed")
+    return {"ops_per_s": v.value, "source": "measured: LOP3 throughput microbenchmark "
+            "(spin-glass_b200/csrc/int_peak.cu), best of 5, in this run"}
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the sweep kernel from the committed ncu summary."""
+    f = ROOT / "profiles" / "pt_resident_L16_production.json"
+    if not f.exists():
+        return None
+    try:
+        return json.loads(f.read_text()).get("dram_bytes_per_launch")
+    except (OSError, ValueError):
+        return None
+
+
+def cpu_sample(target_s: float, n_threads: int = 0) -> dict:
+    """The CPU oracle (a scalar port of the reference's update rule, OpenMP over
+    planes) on the same workload, for a bounded number of sweeps."""
+    from oracle import oracle as orc
+    orc.build()
+    betas = 1.0 / (T_MIN * (T_MAX / T_MIN) ** (np.arange(T) / (T - 1)))
+    spins, bonds = orc.init(L, W, NCOPY, T, SEED)
+    obs = orc.Observables(L, W, NCOPY, T)
+    sweeps, t0 = 0, time.perf_counter()
+    while True:
+        orc.run(spins, bonds, L=L, betas=betas, H=0.0, seed=SEED, sweep0=SWEEP0 + sweeps,
+                n_sweeps=1, sweeps_per_swap=1, sweeps_per_meas=1, obs=obs, n_threads=n_threads)
+        sweeps += 1
+        el = time.perf_counter() - t0
+        if el >= target_s:
+            break
+    cores = n_threads or os.cpu_count()
+    return {"value": sweeps * attempts_per_sweep() / (el * 1e9), "unit": METRIC, "cores": cores,
+            "kind": "port",
+            "sample": f"{sweeps} full sweeps (+exchange, +measurement) of the same workload, "
+                      f"{el:.1f} s, {cores} OpenMP threads"}
+
+
+def run_reference(args, rank: int, world: int) -> None:
+    if rank != 0:
+        return
+    from oracle import oracle as orc
+    orc.build()
+    betas = 1.0 / (T_MIN * (T_MAX / T_MIN) ** (np.arange(T) / (T - 1)))
+    spins, bonds = orc.init(L, W, NCOPY, T, SEED)
+    obs = orc.Observables(L, W, NCOPY, T)
+    # one step = one sweep of the workload (a bounded sample of a 1024-sweep section)
+    for k in range(args.warmup):
+        orc.run(spins, bonds, L=L, betas=betas, H=0.0, seed=SEED, sweep0=SWEEP0 + k,
+                n_sweeps=1, sweeps_per_swap=1, sweeps_per_meas=1, obs=obs)
+    t0 = time.perf_counter()
+    orc.run(spins, bonds, L=L, betas=betas, H=0.0, seed=SEED, sweep0=SWEEP0 + args.warmup,
+            n_sweeps=args.steps, sweeps_per_swap=1, sweeps_per_meas=1, obs=obs)
+    el = time.perf_counter() - t0
+    value = args.steps * attempts_per_sweep() / (el * 1e9)
+    cores = os.cpu_count()
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": workload_config(world),
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "port",
+                             "sample": f"{args.steps} sweeps of the workload (1 sweep per step), "
+                                       f"{cores} OpenMP threads; the reference itself has no "
+                                       "CPU implementation of this path"},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank: int, world: int, dist) -> None:
+    import torch
+    csg = _package()
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    seed = SEED + rank
+    betas = 1.0 / (T_MIN * (T_MAX / T_MIN) ** (np.arange(T) / (T - 1)))
+    cfg, _keep = csg.make_config(L, W, NCOPY, betas, seed=seed, sweeps_per_swap=1,
+                                 sweeps_per_meas=1, meas_start=0)
+    N = L ** 3
+    spins = torch.empty(W * NCOPY * T * N, dtype=torch.int32, device=dev)
+    bonds = torch.empty(W * 3 * N, dtype=torch.int32, device=dev)
+    z64 = lambda *s: torch.zeros(s, dtype=torch.int64, device=dev)
+    acc = {"e_sum": z64(W, NCOPY, T, 32), "q_sum": z64(W, T, 32), "q2_sum": z64(W, T, 32),
+           "q4_sum": z64(W, T, 32, 2), "hist": torch.zeros((T, N + 1), dtype=torch.int32, device=dev),
+           "e_last": torch.zeros((W, NCOPY, T, 32), dtype=torch.int32, device=dev),
+           "d_last": torch.zeros((W, T, 32), dtype=torch.int32, device=dev), "boundary": z64(1)}
+    obs = csg.DeviceObs(**{k: v.data_ptr() for k, v in acc.items()})
+    stream = torch.cuda.current_stream(dev)
+    csg.init_device(cfg, spins.data_ptr(), bonds.data_ptr(), stream.cuda_stream)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device=dev)  # 256 MiB > L2
+
+    def step(k):
+        csg.run_device(cfg, spins.data_ptr(), bonds.data_ptr(), obs, SWEEP0 + k * SWEEPS_PER_STEP,
+                       SWEEPS_PER_STEP, stream.cuda_stream)
+
+    for k in range(args.warmup):
+        step(k)
+    torch.cuda.synchronize(dev)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.fill_(k)
+            ev[k][0].record(stream)
+            step(args.warmup + k)
+            ev[k][1].record(stream)
+        torch.cuda.synchronize(dev)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    per_launch_ms = [a.elapsed_time(b) for a, b in ev]
+    t_ms = sum(per_launch_ms)
+    if dist is not None:
+        t = torch.tensor([t_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ms = float(t.item())
+    boundary = int(acc["boundary"].item())
+    total_attempts = world * args.steps * SWEEPS_PER_STEP * attempts_per_sweep()
+    value = total_attempts / (t_ms * 1e6)
+
+    # ---- end to end through the engine API: host state in, observables out ----
+    e2e = run_e2e(csg, torch, betas, seed, args)
+    if dist is not None:
+        t = torch.tensor([e2e["seconds"]], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e["value"] = world * e2e["attempts"] / (float(t.item()) * 1e9)
+
+    if rank != 0:
+        return
+    mean_launch_s = (sum(per_launch_ms) / len(per_launch_ms)) * 1e-3
+    word_updates = SWEEPS_PER_STEP * W * NCOPY * T * N
+    achieved = word_updates * OPS_PER_WORD_UPDATE / mean_launch_s
+    peak = int_peak_ops()
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded +-J disorder, uniform random initial spins)",
+            "config": workload_config(world),
+            "roofline": {"bound": "int", "achieved": achieved / 1e12, "peak": peak["ops_per_s"] / 1e12,
+                         "unit": "Tops/s (32-bit integer logic)",
+                         "frac": achieved / peak["ops_per_s"], "traffic": profile_traffic(),
+                         "ops_per_attempt": OPS_PER_WORD_UPDATE / 32, "peak_source": peak["source"]},
+            "e2e": {"value": e2e["value"], "unit": METRIC,
+                    "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]},
+            "gpu_launches": args.steps,
+            "exchange_boundary_cases": boundary,
+            "clocks": clk.summary()}
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_sample(args.cpu_seconds)
+    print(json.dumps(line), flush=True)
+
+
+def run_e2e(csg, torch, betas, seed, args) -> dict:
+    """csg_set_state (pinned host -> device), csg_run (one section),
+    csg_get_observables (device -> host) per step, wall-clock timed."""
+    N = L ** 3
+    hs = torch.empty(W * NCOPY * T * N, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    hb = torch.empty(W * 3 * N, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    with csg.Engine(L, W, NCOPY, betas, seed=seed, sweeps_per_swap=1, sweeps_per_meas=1) as eng:
+        eng.init_lattice()
+        s, b, _ = eng.get_state()
+        hs[:] = s.ravel()
+        hb[:] = b.ravel()
+        spins_h, bonds_h = hs.reshape(s.shape), hb.reshape(b.shape)
+        eng.set_state(spins_h, bonds_h, SWEEP0)
+        eng.run(SWEEPS_PER_STEP)
+        eng.observables()
+        t0 = time.perf_counter()
+        d2h = 0
+        for k in range(args.steps):
+            eng.set_state(spins_h, bonds_h, SWEEP0 + k * SWEEPS_PER_STEP)
+            eng.run(SWEEPS_PER_STEP)
+            o = eng.observables()
+            d2h = sum(getattr(o, f).nbytes for f in ("e_sum", "m_sum", "q_sum", "q2_sum", "q4_sum",
+                                                     "hist", "e_last", "m_last", "d_last",
+                                                     "swap_acc")) + 8
+        el = time.perf_counter() - t0
+    attempts = args.steps * SWEEPS_PER_STEP * attempts_per_sweep()
+    return {"value": attempts / (el * 1e9), "seconds": el, "attempts": attempts,
+            "h2d": int(hs.nbytes + hb.nbytes), "d2h": int(d2h)}
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -14,6 +14,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libcsg.so"
 CLI = PKG / "csg"
+PEAK = PKG / "libcsg_peak.so"
 
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -50,9 +51,18 @@ def build_cli(force: bool = False) -> pathlib.Path | None:
     return CLI
 
 
+def build_peak(force: bool = False) -> pathlib.Path:
+    src = CSRC / "int_peak.cu"
+    if force or _stale(PEAK, [src]):
+        cmd = [NVCC, *ARCH, "-O3", "-Xcompiler", "-fPIC", "-shared", "-o", str(PEAK), str(src)]
+        subprocess.run(cmd, check=True)
+    return PEAK
+
+
 def build(force: bool = False) -> None:
     build_lib(force)
     build_cli(force)
+    build_peak(force)
 
 
 if __name__ == "__main__":
