@@ -248,8 +248,9 @@ def run_ours(args, rank: int, world: int, dist) -> None:
     value = total_attempts / (t_ms * 1e6)
 
     # ---- end to end through the engine API: host state in, observables out ----
-    e2e = run_e2e(csg, torch, betas, seed, args)
-    if dist is not None:
+    e2e = ({"value": None, "seconds": 0.0, "attempts": 0, "h2d": 0, "d2h": 0}
+           if args.no_e2e else run_e2e(csg, torch, betas, seed, args))
+    if dist is not None and not args.no_e2e:
         t = torch.tensor([e2e["seconds"]], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e["value"] = world * e2e["attempts"] / (float(t.item()) * 1e9)
@@ -317,6 +318,8 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true",
+                    help="skip the end-to-end leg (profiling runs)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

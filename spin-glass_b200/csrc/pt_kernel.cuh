@@ -221,10 +221,12 @@ __device__ __forceinline__ uint32_t flip_h0(uint32_t sa, uint32_t ca, uint32_t s
 __device__ __forceinline__ uint32_t flip_gen(uint32_t s0, uint32_t sa, uint32_t ca, uint32_t sb,
                                              uint32_t cb, uint32_t r, const uint32_t* thr,
                                              const uint8_t* ucut) {
+    // U = sa + sb + 2(ca + cb): U >= 4 needs both carries, or one carry and
+    // both sum bits; U >= 5 and U >= 6 need both carries.
     const uint32_t v = sa | sb;
-    const uint32_t ge4 = ca & cb;
-    const uint32_t ge[7] = {0xFFFFFFFFu, ca | cb | v, ca | cb | (sa & sb), maj3(ca, cb, v), ge4,
-                            ge4 & v, ge4 & sa & sb};
+    const uint32_t cc = ca & cb;
+    const uint32_t ge[7] = {0xFFFFFFFFu, ca | cb | v, ca | cb | (sa & sb), maj3(ca, cb, v),
+                            cc | ((ca | cb) & sa & sb), cc & v, cc & sa & sb};
     uint32_t g0 = 0, g1 = 0;
 #pragma unroll
     for (int U = 6; U >= 0; --U) {
