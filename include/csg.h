@@ -191,6 +191,23 @@ int csg_query_plan(const csg_config* cfg, csg_plan* out);
  * NULL or quads_per_cta == 0 restores the automatic plan. */
 int csg_set_plan_override(const csg_plan* plan);
 
+/* No counterpart in the reference.  The observable records of
+ * csg_obs_records for a state held in the caller's device memory, without
+ * allocating anything: for callers whose device memory all belongs to their
+ * own pool or budget (a framework's caching allocator, a server admitting
+ * work against a fixed budget), where a library's cudaMalloc could fail and
+ * its cudaFree would synchronise the device.  spins/bonds (canonical layout)
+ * and rec ([32W][T][11] floats) are device pointers; the kernels are queued
+ * on `stream` and the caller synchronises.  The intermediate integers live in
+ * one fixed 16 MiB device array per GPU, held until the process exits; a call
+ * needs W*T*32*(5+3L) ints of it and larger states are rejected with
+ * CSG_ERR_UNSUPPORTED.  The first call on a device looks up that array's
+ * device address (make it before any stream capture).  All calls share the
+ * array: calls that overlap on the GPU (other streams, other threads) race.
+ * Every element a call reads is written by that call first. */
+int csg_obs_records_noalloc(const csg_config* cfg, const uint32_t* spins, const uint32_t* bonds,
+                            float* rec, size_t n_floats, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

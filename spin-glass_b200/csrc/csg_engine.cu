@@ -23,6 +23,15 @@ int fail(int code, const std::string& msg) {
     return code;
 }
 
+}  // namespace
+
+// Lets other translation units of the library report through csg_last_error().
+namespace csg_detail {
+__attribute__((visibility("hidden"))) void set_last_error(const std::string& msg) { g_err = msg; }
+}  // namespace csg_detail
+
+namespace {
+
 #define CSG_CUDA(call)                                                                    \
     do {                                                                                  \
         const cudaError_t e_ = (call);                                                    \
