@@ -121,19 +121,19 @@ KernelFn select_kernel(int L, bool gen) {
     }
 }
 
-size_t smem_for(int L, int Qc) {
+size_t smem_for(int L, int Qc, bool has_m, bool gen) {
     switch (L) {
-        case 4: return csg::SmemMap<4>::bytes(Qc);
-        case 6: return csg::SmemMap<6>::bytes(Qc);
-        case 8: return csg::SmemMap<8>::bytes(Qc);
-        case 10: return csg::SmemMap<10>::bytes(Qc);
-        case 12: return csg::SmemMap<12>::bytes(Qc);
-        case 14: return csg::SmemMap<14>::bytes(Qc);
-        case 16: return csg::SmemMap<16>::bytes(Qc);
-        case 18: return csg::SmemMap<18>::bytes(Qc);
-        case 20: return csg::SmemMap<20>::bytes(Qc);
-        case 22: return csg::SmemMap<22>::bytes(Qc);
-        case 24: return csg::SmemMap<24>::bytes(Qc);
+        case 4: return csg::SmemMap<4>::bytes(Qc, has_m, gen);
+        case 6: return csg::SmemMap<6>::bytes(Qc, has_m, gen);
+        case 8: return csg::SmemMap<8>::bytes(Qc, has_m, gen);
+        case 10: return csg::SmemMap<10>::bytes(Qc, has_m, gen);
+        case 12: return csg::SmemMap<12>::bytes(Qc, has_m, gen);
+        case 14: return csg::SmemMap<14>::bytes(Qc, has_m, gen);
+        case 16: return csg::SmemMap<16>::bytes(Qc, has_m, gen);
+        case 18: return csg::SmemMap<18>::bytes(Qc, has_m, gen);
+        case 20: return csg::SmemMap<20>::bytes(Qc, has_m, gen);
+        case 22: return csg::SmemMap<22>::bytes(Qc, has_m, gen);
+        case 24: return csg::SmemMap<24>::bytes(Qc, has_m, gen);
         default: return 0;
     }
 }
@@ -150,6 +150,12 @@ csg_plan g_override = {0, 0, 0, 0};
 
 int prepare_kernel(KernelFn fn, size_t smem, int K) {
     CSG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // Ask for the smallest shared-memory carve-out that holds the CTA (plus the
+    // 1 KB the system reserves per CTA) so that the rest of the SM's 256 KB
+    // stays L1 for the bonds.
+    const int pct = (int)((smem + 1024) * 100 / (228 * 1024));
+    CSG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  pct < 100 ? pct : 100));
     if (K > 8) CSG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     return CSG_OK;
 }
@@ -177,6 +183,7 @@ int make_plan(const csg_config& cfg, bool gen, Plan& out) {
     const int L = cfg.dims.L, W = cfg.dims.n_words;
     const int G = cfg.dims.n_copies * cfg.dims.n_temps / 4;
     const int tpq = csg::tpq_for(L);
+    const bool has_m = gen || (cfg.flags & CSG_MEASURE_M);
     KernelFn fn = select_kernel(L, gen);
     if (!fn) return fail(CSG_ERR_UNSUPPORTED, "no kernel for L");
     {
@@ -187,7 +194,7 @@ int make_plan(const csg_config& cfg, bool gen, Plan& out) {
             out.Qc = Qc;
             out.K = G / Qc;
             out.TPQ = tpq;
-            out.smem = smem_for(L, Qc);
+            out.smem = smem_for(L, Qc, has_m, gen);
             if (out.K > 16 || out.smem > kMaxSmem || Qc * tpq > csg::kMaxThreads)
                 return fail(CSG_ERR_UNSUPPORTED, "plan override exceeds device limits");
             return prepare_kernel(fn, out.smem, out.K);
@@ -203,7 +210,7 @@ int make_plan(const csg_config& cfg, bool gen, Plan& out) {
         pl.Qc = Qc;
         pl.K = G / Qc;
         pl.TPQ = tpq;
-        pl.smem = smem_for(L, Qc);
+        pl.smem = smem_for(L, Qc, has_m, gen);
         if (pl.K > 16 || pl.smem > kMaxSmem || Qc * tpq > csg::kMaxThreads) continue;
         if (prepare_kernel(fn, pl.smem, pl.K) != CSG_OK) continue;
         cudaLaunchConfig_t lc;

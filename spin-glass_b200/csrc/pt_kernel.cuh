@@ -97,7 +97,9 @@ struct LCfg {
     static constexpr int SPT = (NH + TPQ - 1) / TPQ;          // sites per thread per colour
     static constexpr int NLV = bit_length(6 * SPT);           // energy counter levels
     static constexpr int MPT = (N + 4 * TPQ - 1) / (4 * TPQ); // 4-site groups per thread
-    static constexpr int NLD = bit_length(4 * MPT);           // overlap counter levels
+    static constexpr int NLD = bit_length(4 * MPT);           // magnetisation counter levels
+    static constexpr int MPH = (NH + 4 * TPQ - 1) / (4 * TPQ); // 4-site groups per half lattice
+    static constexpr int NLH = bit_length(4 * MPH);           // overlap counter levels
 };
 
 __device__ __forceinline__ uint32_t maj3(uint32_t a, uint32_t b, uint32_t c) {
@@ -239,13 +241,18 @@ __device__ __forceinline__ uint32_t flip_gen(uint32_t s0, uint32_t sa, uint32_t 
 }
 
 // Shared-memory layout of one CTA (dynamic):
-//   uint4 quads[Qc][N]; int sE[Qc*4][32]; int sM[Qc*4][32]; int sD[Qc*4][32];
-//   uint32 sMask[2*Qc]; uint32 sThr[Qc*4][2][7]; uint8 sUcut[Qc*4][2]
+//   uint4 quads[Qc][N]; int sE[Qc*4][32]; int sD[Qc*4][32];
+//   int sM[Qc*4][32]                      (only with magnetisations)
+//   uint32 sThr[Qc*4][2][7]; uint8 sUcut[Qc*4][2]   (only for H != 0)
+// The exchange masks of a round live in the first 2*Qc words of sD, which is
+// cleared again before the overlap counts are added.  At L=16 with 3 quads the
+// H=0 layout is 195 KB, under the 196 KB carve-out, so the 48 KB of bonds of
+// the word stay in L1.
 template <int L>
 struct SmemMap {
-    static __host__ __device__ size_t bytes(int Qc) {
-        return (size_t)Qc * LCfg<L>::N * 16 + (size_t)Qc * 4 * 32 * 4 * 3 + (size_t)Qc * 2 * 4 +
-               (size_t)Qc * 4 * 14 * 4 + (size_t)Qc * 4 * 2 + 16;
+    static __host__ __device__ size_t bytes(int Qc, bool has_m, bool gen) {
+        return (size_t)Qc * LCfg<L>::N * 16 + (size_t)Qc * 4 * 32 * 4 * (has_m ? 3 : 2) +
+               (gen ? (size_t)Qc * 4 * 14 * 4 + (size_t)Qc * 4 * 2 : 0);
     }
 };
 
@@ -253,7 +260,7 @@ template <int L, bool GEN_H>
 __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_constant__ PtParams P) {
     using CF = LCfg<L>;
     constexpr int N = CF::N, NH = CF::NH, LH = CF::LH, TPQ = CF::TPQ;
-    constexpr int NLV = CF::NLV, NLD = CF::NLD;
+    constexpr int NLV = CF::NLV, NLD = CF::NLD, NLH = CF::NLH;
 
     cgx::cluster_group cluster = cgx::this_cluster();
     const int rank = (int)cluster.block_rank();
@@ -270,11 +277,12 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint4* S = reinterpret_cast<uint4*>(smem_raw);
+    const bool has_M = GEN_H || (P.flags & kFlagMeasureM);
     int* sE = reinterpret_cast<int*>(smem_raw + (size_t)Qc * N * 16);
-    int* sM = sE + Qc * 4 * 32;
-    int* sD = sM + Qc * 4 * 32;
-    uint32_t* sMask = reinterpret_cast<uint32_t*>(sD + Qc * 4 * 32);
-    uint32_t* sThr = sMask + 2 * Qc;
+    int* sD = sE + Qc * 4 * 32;
+    int* sM = sD + Qc * 4 * 32;  // valid only when has_M
+    uint32_t* sMask = reinterpret_cast<uint32_t*>(sD);
+    uint32_t* sThr = reinterpret_cast<uint32_t*>(sM + (has_M ? Qc * 4 * 32 : 0));
     uint8_t* sUcut = reinterpret_cast<uint8_t*>(sThr + Qc * 4 * 14);
 
     // ---- load this CTA's quads (contiguous in global memory) ----
@@ -283,17 +291,19 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
         const uint4* src = reinterpret_cast<const uint4*>(P.spins) + qbase;
         for (int i = tid; i < Qc * N; i += nthreads) S[i] = src[i];
     }
-    for (int i = tid; i < Qc * 4 * 14; i += nthreads) {
-        const int pl = i / 14, k = i - pl * 14;
-        const int gg = rank * Qc + pl / 4;
-        const int t = 4 * (gg % Q) + (pl & 3);
-        sThr[i] = P.tab.thr[t][k / 7][k % 7];
-    }
-    for (int i = tid; i < Qc * 4 * 2; i += nthreads) {
-        const int pl = i / 2;
-        const int gg = rank * Qc + pl / 4;
-        const int t = 4 * (gg % Q) + (pl & 3);
-        sUcut[i] = P.tab.ucut[t][i & 1];
+    if constexpr (GEN_H) {
+        for (int i = tid; i < Qc * 4 * 14; i += nthreads) {
+            const int pl = i / 14, k = i - pl * 14;
+            const int gg = rank * Qc + pl / 4;
+            const int t = 4 * (gg % Q) + (pl & 3);
+            sThr[i] = P.tab.thr[t][k / 7][k % 7];
+        }
+        for (int i = tid; i < Qc * 4 * 2; i += nthreads) {
+            const int pl = i / 2;
+            const int gg = rank * Qc + pl / 4;
+            const int t = 4 * (gg % Q) + (pl & 3);
+            sUcut[i] = P.tab.ucut[t][i & 1];
+        }
     }
     uint32_t th0[4], th1[4], th2[4];
 #pragma unroll
@@ -319,8 +329,8 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
         const bool need_M = need_E && (GEN_H || (do_meas && (P.flags & kFlagMeasureM)));
         const uint32_t s32 = (uint32_t)s;
 
-        if (need_E)
-            for (int i = tid; i < Qc * 4 * 32 * 3; i += nthreads) sE[i] = 0;  // sE, sM, sD
+        if (need_E)  // sE, sD and (if present) sM are contiguous
+            for (int i = tid; i < Qc * 4 * 32 * (has_M ? 3 : 2); i += nthreads) sE[i] = 0;
 
         uint32_t ecnt[4][NLV];
 #pragma unroll
@@ -514,6 +524,8 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
             // rounds the pair (3 of quad g, 0 of quad g+1) crosses quads, so
             // each quad writes back only the words its own pairs touch
             const uint32_t mA = sMask[2 * j], mB = sMask[2 * j + 1];
+            __syncthreads();  // masks read: their words of sD go back to zero
+            for (int i = tid; i < 2 * Qc; i += nthreads) sD[i] = 0;
             if (par == 0) {
                 if (mA | mB) {
                     for (int n = lt; n < N; n += TPQ) {
@@ -570,43 +582,48 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
             }
             if (C == 2) {
                 if (!do_swap) cluster.sync();  // partner copies finished the sweep
-                if (c == 0) {
-                    const int g2 = g + Q, r2 = g2 / Qc, j2 = g2 - r2 * Qc;
-                    const uint4* Sp = cluster.map_shared_rank(S + (size_t)j2 * N, r2);
-                    uint32_t dc[4][NLD];
+                // Overlap of quad q: the copy-0 team counts the colour-0 sites,
+                // the copy-1 team the colour-1 sites; both add into the counts of
+                // the copy-0 quad's CTA.
+                const int gp = c == 0 ? g + Q : g - Q;
+                const int rp = gp / Qc, jp = gp - rp * Qc;
+                const uint4* Sp = cluster.map_shared_rank(S + (size_t)jp * N, rp);
+                const uint4* Sh = Sq + c * NH;
+                Sp += c * NH;
+                uint32_t dc[4][NLH];
 #pragma unroll
-                    for (int k = 0; k < 4; ++k)
+                for (int k = 0; k < 4; ++k)
 #pragma unroll
-                        for (int l = 0; l < NLD; ++l) dc[k][l] = 0;
+                    for (int l = 0; l < NLH; ++l) dc[k][l] = 0;
 #pragma unroll 1
-                    for (int n = lt; n < N; n += 4 * TPQ) {
-                        uint4 v[4];
+                for (int n = lt; n < NH; n += 4 * TPQ) {
+                    uint4 v[4];
 #pragma unroll
-                        for (int u = 0; u < 4; ++u) {
-                            const int nn = n + u * TPQ;
-                            if (nn < N) {
-                                const uint4 a = Sq[nn], b = Sp[nn];
-                                v[u] = make_uint4(a.x ^ b.x, a.y ^ b.y, a.z ^ b.z, a.w ^ b.w);
-                            } else {
-                                v[u] = make_uint4(0, 0, 0, 0);
-                            }
+                    for (int u = 0; u < 4; ++u) {
+                        const int nn = n + u * TPQ;
+                        if (nn < NH) {
+                            const uint4 a = Sh[nn], b = Sp[nn];
+                            v[u] = make_uint4(a.x ^ b.x, a.y ^ b.y, a.z ^ b.z, a.w ^ b.w);
+                        } else {
+                            v[u] = make_uint4(0, 0, 0, 0);
                         }
-                        vc_add4<NLD>(dc[0], v[0].x, v[1].x, v[2].x, v[3].x);
-                        vc_add4<NLD>(dc[1], v[0].y, v[1].y, v[2].y, v[3].y);
-                        vc_add4<NLD>(dc[2], v[0].z, v[1].z, v[2].z, v[3].z);
-                        vc_add4<NLD>(dc[3], v[0].w, v[1].w, v[2].w, v[3].w);
                     }
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        const int cnt = column_count<NLD>(dc[k], lane);
-                        atomicAdd(&sD[(j * 4 + k) * 32 + lane], cnt);
-                    }
+                    vc_add4<NLH>(dc[0], v[0].x, v[1].x, v[2].x, v[3].x);
+                    vc_add4<NLH>(dc[1], v[0].y, v[1].y, v[2].y, v[3].y);
+                    vc_add4<NLH>(dc[2], v[0].z, v[1].z, v[2].z, v[3].z);
+                    vc_add4<NLH>(dc[3], v[0].w, v[1].w, v[2].w, v[3].w);
                 }
-                __syncthreads();
+                int* dst = c == 0 ? sD + j * 4 * 32 : cluster.map_shared_rank(sD + jp * 4 * 32, rp);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int cnt = column_count<NLH>(dc[k], lane);
+                    atomicAdd(&dst[k * 32 + lane], cnt);
+                }
+                cluster.sync();  // all counts in; partner planes may be modified again
                 for (int i = tid; i < Qc * 4 * 32; i += nthreads) {
                     const int pl = i >> 5, b = i & 31;
                     const int gg = rank * Qc + (pl >> 2);
-                    if (gg >= Q) continue;  // copy-1 quads: counted by the copy-0 owner
+                    if (gg >= Q) continue;  // copy-1 quads: counted in the copy-0 owner
                     const int t = 4 * gg + (pl & 3);
                     const int D = sD[i];
                     const long long Qv = (long long)N - 2LL * D;
@@ -624,8 +641,8 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
                     if (P.hist) atomicAdd(&P.hist[(size_t)t * (N + 1) + D], 1u);
                     if (P.d_last) P.d_last[o] = D;
                 }
-                cluster.sync();  // partner planes may be modified again
             }
+            __syncthreads();  // sE / sD are cleared at the start of the next sweep
         }
     }
 
