@@ -54,10 +54,11 @@ def attempts_per_sweep() -> int:
     return L ** 3 * W * 32 * NCOPY * T
 
 
-def workload_config(n_gpus: int) -> dict:
+def workload_config(n_gpus: int, swap_every: int = 1, measure_every: int = 1) -> dict:
     return {"workload": "plain PT engine, production size", "L": L, "samples": 32 * W,
             "copies": NCOPY, "temperatures": T, "T_range": [T_MIN, T_MAX],
-            "sweeps_per_step": SWEEPS_PER_STEP, "swap_every": 1, "measure_every": 1,
+            "sweeps_per_step": SWEEPS_PER_STEP, "swap_every": swap_every,
+            "measure_every": measure_every,
             "field_H": 0.0, "l2": "flushed between timed steps (256 MiB write)",
             "parallelism": f"sample shards x{n_gpus}"}
 
@@ -200,8 +201,8 @@ def run_ours(args, rank: int, world: int, dist) -> None:
     dev = torch.device("cuda", local)
     seed = SEED + rank
     betas = 1.0 / (T_MIN * (T_MAX / T_MIN) ** (np.arange(T) / (T - 1)))
-    cfg, _keep = csg.make_config(L, W, NCOPY, betas, seed=seed, sweeps_per_swap=1,
-                                 sweeps_per_meas=1, meas_start=0)
+    cfg, _keep = csg.make_config(L, W, NCOPY, betas, seed=seed, sweeps_per_swap=args.swap_every,
+                                 sweeps_per_meas=args.measure_every, meas_start=0)
     N = L ** 3
     spins = torch.empty(W * NCOPY * T * N, dtype=torch.int32, device=dev)
     bonds = torch.empty(W * 3 * N, dtype=torch.int32, device=dev)
@@ -265,7 +266,7 @@ def run_ours(args, rank: int, world: int, dist) -> None:
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic (seeded +-J disorder, uniform random initial spins)",
-            "config": workload_config(world),
+            "config": workload_config(world, args.swap_every, args.measure_every),
             "roofline": {"bound": "int", "achieved": achieved / 1e12, "peak": peak["ops_per_s"] / 1e12,
                          "unit": "Tops/s (32-bit integer logic)",
                          "frac": achieved / peak["ops_per_s"], "traffic": profile_traffic(),
@@ -286,7 +287,8 @@ def run_e2e(csg, torch, betas, seed, args) -> dict:
     N = L ** 3
     hs = torch.empty(W * NCOPY * T * N, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
     hb = torch.empty(W * 3 * N, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
-    with csg.Engine(L, W, NCOPY, betas, seed=seed, sweeps_per_swap=1, sweeps_per_meas=1) as eng:
+    with csg.Engine(L, W, NCOPY, betas, seed=seed, sweeps_per_swap=args.swap_every,
+                    sweeps_per_meas=args.measure_every) as eng:
         eng.init_lattice()
         s, b, _ = eng.get_state()
         hs[:] = s.ravel()
@@ -318,6 +320,8 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--swap-every", type=int, default=1, help="sweeps per exchange round (0: none)")
+    ap.add_argument("--measure-every", type=int, default=1, help="sweeps per measurement (0: none)")
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the end-to-end leg (profiling runs)")
     args = ap.parse_args()

@@ -92,7 +92,10 @@ typedef struct csg_observables {
 } csg_observables;
 
 /* Device-side accumulators for csg_pt_run_device (device pointers, any may be
- * NULL).  swap_log row k holds global exchange round swap_round0 + k. */
+ * NULL).  swap_log row k holds global exchange round swap_round0 + k.  On the
+ * device q4_sum[..][0] accumulates Q^4 mod 2^32 and q4_sum[..][1] accumulates
+ * floor(Q^4 / 2^32); the total is q4_sum[1]*2^32 + q4_sum[0]
+ * (csg_get_observables returns it as a 128-bit value). */
 typedef struct csg_device_obs {
     int64_t* e_sum;
     int64_t* m_sum;

@@ -553,6 +553,14 @@ int csg_get_observables(csg_engine* e, csg_observables* out) {
     uint64_t b = 0;
     CSG_CUDA(cudaMemcpyAsync(&b, e->boundary, 8, cudaMemcpyDeviceToHost, e->stream));
     CSG_CUDA(cudaStreamSynchronize(e->stream));
+    if (out->q4_sum)  // device split {sum of low 32 bits, sum of the rest} -> 128-bit
+        for (size_t i = 0; i < e->n_q; ++i) {
+            const uint64_t low = out->q4_sum[2 * i], high = out->q4_sum[2 * i + 1];
+            const uint64_t shifted = high << 32;  // total = high * 2^32 + low
+            const uint64_t lo = shifted + low;
+            out->q4_sum[2 * i] = lo;
+            out->q4_sum[2 * i + 1] = (high >> 32) + (lo < shifted ? 1u : 0u);
+        }
     out->boundary = b;
     out->n_meas = e->n_meas;
     out->swap_rounds = e->swap_rounds;

@@ -528,6 +528,7 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
             for (int i = tid; i < 2 * Qc; i += nthreads) sD[i] = 0;
             if (par == 0) {
                 if (mA | mB) {
+#pragma unroll 4
                     for (int n = lt; n < N; n += TPQ) {
                         uint4 v = Sq[n];
                         const uint32_t d0 = (v.x ^ v.y) & mA;
@@ -542,6 +543,7 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
             } else {
                 if (mA) {
                     uint32_t* base = reinterpret_cast<uint32_t*>(Sq);
+#pragma unroll 4
                     for (int n = lt; n < N; n += TPQ) {
                         const uint32_t y = base[4 * n + 1], z = base[4 * n + 2];
                         const uint32_t d = (y ^ z) & mA;
@@ -554,11 +556,26 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
                     uint32_t* nb = reinterpret_cast<uint32_t*>(
                         cluster.map_shared_rank(S + (size_t)j2 * N, r2));
                     uint32_t* base = reinterpret_cast<uint32_t*>(Sq);
-                    for (int n = lt; n < N; n += TPQ) {
-                        const uint32_t a = base[4 * n + 3], b = nb[4 * n];
-                        const uint32_t d = (a ^ b) & mB;
-                        base[4 * n + 3] = a ^ d;
-                        nb[4 * n] = b ^ d;
+                    // chunks of 8 sites: all loads (some from the peer CTA) are in
+                    // flight together before the first store
+                    constexpr int CH = 8;
+                    for (int n0 = lt; n0 < N; n0 += CH * TPQ) {
+                        uint32_t a[CH], b[CH];
+#pragma unroll
+                        for (int u = 0; u < CH; ++u) {
+                            const int n = n0 + u * TPQ;
+                            a[u] = n < N ? base[4 * n + 3] : 0u;
+                            b[u] = n < N ? nb[4 * n] : 0u;
+                        }
+#pragma unroll
+                        for (int u = 0; u < CH; ++u) {
+                            const int n = n0 + u * TPQ;
+                            if (n < N) {
+                                const uint32_t d = (a[u] ^ b[u]) & mB;
+                                base[4 * n + 3] = a[u] ^ d;
+                                nb[4 * n] = b[u] ^ d;
+                            }
+                        }
                     }
                 }
             }
@@ -573,10 +590,12 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
                 const int gg = rank * Qc + (pl >> 2);
                 const int cc = gg / Q, t = 4 * (gg - cc * Q) + (pl & 3);
                 const size_t o = (((size_t)w * C + cc) * T + t) * 32 + b;
-                if (P.e_sum) P.e_sum[o] += sE[i];
+                if (P.e_sum) atomicAdd(reinterpret_cast<unsigned long long*>(P.e_sum + o),
+                                       (unsigned long long)(long long)sE[i]);
                 if (P.e_last) P.e_last[o] = sE[i];
                 if (need_M) {
-                    if (P.m_sum) P.m_sum[o] += sM[i];
+                    if (P.m_sum) atomicAdd(reinterpret_cast<unsigned long long*>(P.m_sum + o),
+                                           (unsigned long long)(long long)sM[i]);
                     if (P.m_last) P.m_last[o] = sM[i];
                 }
             }
@@ -595,7 +614,7 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
                 for (int k = 0; k < 4; ++k)
 #pragma unroll
                     for (int l = 0; l < NLH; ++l) dc[k][l] = 0;
-#pragma unroll 1
+#pragma unroll 2
                 for (int n = lt; n < NH; n += 4 * TPQ) {
                     uint4 v[4];
 #pragma unroll
@@ -629,14 +648,15 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
                     const long long Qv = (long long)N - 2LL * D;
                     const unsigned long long q2 = (unsigned long long)(Qv * Qv);
                     const size_t o = ((size_t)w * T + t) * 32 + b;
-                    if (P.q_sum) P.q_sum[o] += Qv;
-                    if (P.q2_sum) P.q2_sum[o] += (long long)q2;
-                    if (P.q4_sum) {
+                    if (P.q_sum)
+                        atomicAdd(reinterpret_cast<unsigned long long*>(P.q_sum + o),
+                                  (unsigned long long)Qv);
+                    if (P.q2_sum)
+                        atomicAdd(reinterpret_cast<unsigned long long*>(P.q2_sum + o), q2);
+                    if (P.q4_sum) {  // Q^4 as sum of low 32 bits and sum of the rest
                         const unsigned long long lo = q2 * q2, hi = __umul64hi(q2, q2);
-                        unsigned long long* a = P.q4_sum + 2 * o;
-                        const unsigned long long old = a[0];
-                        a[0] = old + lo;
-                        a[1] += hi + (a[0] < old ? 1ull : 0ull);
+                        atomicAdd(P.q4_sum + 2 * o, lo & 0xFFFFFFFFull);
+                        atomicAdd(P.q4_sum + 2 * o + 1, (lo >> 32) | (hi << 32));
                     }
                     if (P.hist) atomicAdd(&P.hist[(size_t)t * (N + 1) + D], 1u);
                     if (P.d_last) P.d_last[o] = D;
