@@ -26,6 +26,7 @@
 #include <cooperative_groups.h>
 
 #include <cstdint>
+#include <type_traits>
 
 #include "philox.cuh"
 
@@ -338,85 +339,94 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
 #pragma unroll
             for (int l = 0; l < NLV; ++l) ecnt[k][l] = 0;
 
-#pragma unroll 1
-        for (int p = 0; p < 2; ++p) {
-            const bool acc_e = need_E && p == 1;
+        // one colour of the checkerboard; ACC: also add the post-flip
+        // unsatisfied-bond counts into the energy counters
+        auto colour_pass = [&](const int p, auto acc_tag) {
+            constexpr bool ACC = decltype(acc_tag)::value;
             uint4* Sc = Sq + p * NH;
             const uint4* So = Sq + (1 - p) * NH;
             const uint32_t* Fc = Fw + p * NH;
             const uint32_t* Fo = Fw + (1 - p) * NH;
 #pragma unroll 1
-            for (int n0 = lt; n0 < NH; n0 += 2 * TPQ) {
-                uint32_t wA[4][4], wB[4][4];
-                bool hasB = false;
-#pragma unroll
-                for (int sidx = 0; sidx < 2; ++sidx) {
-                    const int n = n0 + sidx * TPQ;
-                    if (sidx == 1 && n >= NH) break;
-                    if (sidx == 1) hasB = true;
-                    const int z = n / (L * LH);
-                    const int rem = n - z * (L * LH);
-                    const int y = rem / LH;
-                    const int h = rem - y * LH;
-                    const int o = (y + z + p) & 1;
-                    const int x = 2 * h + o;
-                    const int hxm = o ? h : (h == 0 ? LH - 1 : h - 1);
-                    const int hxp = o ? (h == LH - 1 ? 0 : h + 1) : h;
-                    const int ym = y == 0 ? L - 1 : y - 1, yp = y == L - 1 ? 0 : y + 1;
-                    const int zm = z == 0 ? L - 1 : z - 1, zp = z == L - 1 ? 0 : z + 1;
-                    const int row = (z * L + y) * LH;
-                    const int nxm = row + hxm, nxp = row + hxp;
-                    const int nym = (z * L + ym) * LH + h, nyp = (z * L + yp) * LH + h;
-                    const int nzm = (zm * L + y) * LH + h, nzp = (zp * L + y) * LH + h;
+                for (int n0 = lt; n0 < NH; n0 += 2 * TPQ) {
+                    uint32_t wA[4][4], wB[4][4];
+                    bool hasB = false;
+    #pragma unroll
+                    for (int sidx = 0; sidx < 2; ++sidx) {
+                        const int n = n0 + sidx * TPQ;
+                        if (sidx == 1 && n >= NH) break;
+                        if (sidx == 1) hasB = true;
+                        const int z = n / (L * LH);
+                        const int rem = n - z * (L * LH);
+                        const int y = rem / LH;
+                        const int h = rem - y * LH;
+                        const int o = (y + z + p) & 1;
+                        const int x = 2 * h + o;
+                        const int hxm = o ? h : (h == 0 ? LH - 1 : h - 1);
+                        const int hxp = o ? (h == LH - 1 ? 0 : h + 1) : h;
+                        const int ym = y == 0 ? L - 1 : y - 1, yp = y == L - 1 ? 0 : y + 1;
+                        const int zm = z == 0 ? L - 1 : z - 1, zp = z == L - 1 ? 0 : z + 1;
+                        const int row = (z * L + y) * LH;
+                        const int nxm = row + hxm, nxp = row + hxp;
+                        const int nym = (z * L + ym) * LH + h, nyp = (z * L + yp) * LH + h;
+                        const int nzm = (zm * L + y) * LH + h, nzp = (zp * L + y) * LH + h;
 
-                    uint4 cv = Sc[n];
-                    const uint4 a0 = So[nxm], a1 = So[nxp], a2 = So[nym], a3 = So[nyp],
-                                a4 = So[nzm], a5 = So[nzp];
-                    const uint32_t f0 = __ldg(Fo + nxm), f1 = __ldg(Fc + n);
-                    const uint32_t f2 = __ldg(Fo + N + nym), f3 = __ldg(Fc + N + n);
-                    const uint32_t f4 = __ldg(Fo + 2 * N + nzm), f5 = __ldg(Fc + 2 * N + n);
-                    const u32x4 r = philox4x32_10((uint32_t)((z * L + y) * L + x), s32, (uint32_t)w,
-                                                  ctr3, P.k0, P.k1);
-                    const uint32_t rr[4] = {r.v0, r.v1, r.v2, r.v3};
-                    uint32_t cw[4] = {cv.x, cv.y, cv.z, cv.w};
-                    const uint32_t n0w[4] = {a0.x, a0.y, a0.z, a0.w}, n1w[4] = {a1.x, a1.y, a1.z, a1.w};
-                    const uint32_t n2w[4] = {a2.x, a2.y, a2.z, a2.w}, n3w[4] = {a3.x, a3.y, a3.z, a3.w};
-                    const uint32_t n4w[4] = {a4.x, a4.y, a4.z, a4.w}, n5w[4] = {a5.x, a5.y, a5.z, a5.w};
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        const uint32_t s0 = cw[k];
-                        const uint32_t u0 = s0 ^ n0w[k] ^ f0, u1 = s0 ^ n1w[k] ^ f1;
-                        const uint32_t u2 = s0 ^ n2w[k] ^ f2, u3 = s0 ^ n3w[k] ^ f3;
-                        const uint32_t u4 = s0 ^ n4w[k] ^ f4, u5 = s0 ^ n5w[k] ^ f5;
-                        const uint32_t sa = u0 ^ u1 ^ u2, ca = maj3(u0, u1, u2);
-                        const uint32_t sb = u3 ^ u4 ^ u5, cb = maj3(u3, u4, u5);
-                        uint32_t fl;
-                        if constexpr (GEN_H)
-                            fl = flip_gen(s0, sa, ca, sb, cb, rr[k], thrq + k * 14, ucq + k * 2);
-                        else
-                            fl = flip_h0(sa, ca, sb, cb, rr[k], th0[k], th1[k], th2[k]);
-                        cw[k] = s0 ^ fl;
-                        uint32_t(&wd)[4] = sidx == 0 ? wA[k] : wB[k];
-                        wd[0] = sa ^ fl;
-                        wd[1] = sb ^ fl;
-                        wd[2] = ca ^ fl;
-                        wd[3] = cb ^ fl;
+                        uint4 cv = Sc[n];
+                        const uint4 a0 = So[nxm], a1 = So[nxp], a2 = So[nym], a3 = So[nyp],
+                                    a4 = So[nzm], a5 = So[nzp];
+                        const uint32_t f0 = __ldg(Fo + nxm), f1 = __ldg(Fc + n);
+                        const uint32_t f2 = __ldg(Fo + N + nym), f3 = __ldg(Fc + N + n);
+                        const uint32_t f4 = __ldg(Fo + 2 * N + nzm), f5 = __ldg(Fc + 2 * N + n);
+                        const u32x4 r = philox4x32_10((uint32_t)((z * L + y) * L + x), s32, (uint32_t)w,
+                                                      ctr3, P.k0, P.k1);
+                        const uint32_t rr[4] = {r.v0, r.v1, r.v2, r.v3};
+                        uint32_t cw[4] = {cv.x, cv.y, cv.z, cv.w};
+                        const uint32_t n0w[4] = {a0.x, a0.y, a0.z, a0.w}, n1w[4] = {a1.x, a1.y, a1.z, a1.w};
+                        const uint32_t n2w[4] = {a2.x, a2.y, a2.z, a2.w}, n3w[4] = {a3.x, a3.y, a3.z, a3.w};
+                        const uint32_t n4w[4] = {a4.x, a4.y, a4.z, a4.w}, n5w[4] = {a5.x, a5.y, a5.z, a5.w};
+    #pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            const uint32_t s0 = cw[k];
+                            const uint32_t u0 = s0 ^ n0w[k] ^ f0, u1 = s0 ^ n1w[k] ^ f1;
+                            const uint32_t u2 = s0 ^ n2w[k] ^ f2, u3 = s0 ^ n3w[k] ^ f3;
+                            const uint32_t u4 = s0 ^ n4w[k] ^ f4, u5 = s0 ^ n5w[k] ^ f5;
+                            const uint32_t sa = u0 ^ u1 ^ u2, ca = maj3(u0, u1, u2);
+                            const uint32_t sb = u3 ^ u4 ^ u5, cb = maj3(u3, u4, u5);
+                            uint32_t fl;
+                            if constexpr (GEN_H)
+                                fl = flip_gen(s0, sa, ca, sb, cb, rr[k], thrq + k * 14, ucq + k * 2);
+                            else
+                                fl = flip_h0(sa, ca, sb, cb, rr[k], th0[k], th1[k], th2[k]);
+                            cw[k] = s0 ^ fl;
+                            if constexpr (ACC) {
+                                uint32_t(&wd)[4] = sidx == 0 ? wA[k] : wB[k];
+                                wd[0] = sa ^ fl;
+                                wd[1] = sb ^ fl;
+                                wd[2] = ca ^ fl;
+                                wd[3] = cb ^ fl;
+                            }
+                        }
+                        Sc[n] = make_uint4(cw[0], cw[1], cw[2], cw[3]);
                     }
-                    Sc[n] = make_uint4(cw[0], cw[1], cw[2], cw[3]);
-                }
-                if (acc_e) {
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        if (hasB)
-                            vc_add_2sites<NLV>(ecnt[k], wA[k][0], wA[k][1], wA[k][2], wA[k][3],
-                                               wB[k][0], wB[k][1], wB[k][2], wB[k][3]);
-                        else
-                            vc_add_site<NLV>(ecnt[k], wA[k][0], wA[k][1], wA[k][2], wA[k][3]);
+                    if constexpr (ACC) {
+    #pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            if (hasB)
+                                vc_add_2sites<NLV>(ecnt[k], wA[k][0], wA[k][1], wA[k][2], wA[k][3],
+                                                   wB[k][0], wB[k][1], wB[k][2], wB[k][3]);
+                            else
+                                vc_add_site<NLV>(ecnt[k], wA[k][0], wA[k][1], wA[k][2], wA[k][3]);
+                        }
                     }
                 }
-            }
-            __syncthreads();
-        }
+        };
+        colour_pass(0, std::false_type{});
+        __syncthreads();
+        if (need_E)
+            colour_pass(1, std::true_type{});
+        else
+            colour_pass(1, std::false_type{});
+        __syncthreads();
 
         if (!need_E) continue;
 
@@ -458,10 +468,24 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
             if (need_M) sM[i] = 2 * sM[i] - N;
         }
 
+        uint32_t mask_keep = 0;  // exchange mask word this thread later finds in sD
         if (do_swap) {
-            cluster.sync();  // energies of every plane of the word are visible
             const long long round = (s + 1) / P.sps - 1;
             const int par = (int)(round & 1);
+            // the uniform of this lane for the warp's first pair does not depend
+            // on the energies: draw it while the cluster barrier is pending
+            auto uniform_for = [&](int pi) {
+                const int gg = rank * Qc + (pi >> 1);
+                const int cc = gg / Q, t = 4 * (gg - cc * Q) + par + 2 * (pi & 1);
+                const u32x4 r = philox4x32_10((uint32_t)(lane >> 1), s32, (uint32_t)w,
+                                              kTagSwap | ((uint32_t)cc << 8) | (uint32_t)t,
+                                              P.k0, P.k1);
+                const uint32_t lo = (lane & 1) ? r.v2 : r.v0;
+                const uint32_t hi = (lane & 1) ? r.v3 : r.v1;
+                return (double)((((unsigned long long)hi << 32) | lo) >> 11) * 0x1p-53;
+            };
+            const double u_first = warp < 2 * Qc ? uniform_for(warp) : 0.0;
+            cluster.sync();  // energies of every plane of the word are visible
             for (int pi = warp; pi < 2 * Qc; pi += nwarps) {
                 const int jj = pi >> 1;
                 const int tq = par + 2 * (pi & 1);
@@ -483,13 +507,7 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
                     }
                     const int e0 = E0[lane], e1 = E1[lane];
                     const int m0 = need_M ? M0[lane] : 0, m1 = need_M ? M1[lane] : 0;
-                    const u32x4 r = philox4x32_10((uint32_t)(lane >> 1), s32, (uint32_t)w,
-                                                  kTagSwap | ((uint32_t)cc << 8) | (uint32_t)t,
-                                                  P.k0, P.k1);
-                    const uint32_t lo = (lane & 1) ? r.v2 : r.v0;
-                    const uint32_t hi = (lane & 1) ? r.v3 : r.v1;
-                    const unsigned long long bits = ((unsigned long long)hi << 32) | lo;
-                    const double u = (double)(bits >> 11) * 0x1p-53;
+                    const double u = pi == warp ? u_first : uniform_for(pi);
                     const double dE = __dsub_rn((double)(e0 - e1), __dmul_rn(P.H, (double)(m0 - m1)));
                     const double delta = __dmul_rn(__dsub_rn(P.tab.beta[t], P.tab.beta[t + 1]), dE);
                     bool acc = true;
@@ -524,8 +542,9 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
             // rounds the pair (3 of quad g, 0 of quad g+1) crosses quads, so
             // each quad writes back only the words its own pairs touch
             const uint32_t mA = sMask[2 * j], mB = sMask[2 * j + 1];
-            __syncthreads();  // masks read: their words of sD go back to zero
-            for (int i = tid; i < 2 * Qc; i += nthreads) sD[i] = 0;
+            // the mask words stay in sD: the thread that later reads word tid
+            // of the overlap counts subtracts them again
+            if (tid < 2 * Qc) mask_keep = sMask[tid];
             if (par == 0) {
                 if (mA | mB) {
 #pragma unroll 4
@@ -644,7 +663,7 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
                     const int gg = rank * Qc + (pl >> 2);
                     if (gg >= Q) continue;  // copy-1 quads: counted in the copy-0 owner
                     const int t = 4 * gg + (pl & 3);
-                    const int D = sD[i];
+                    const int D = (int)((uint32_t)sD[i] - (i == tid ? mask_keep : 0u));
                     const long long Qv = (long long)N - 2LL * D;
                     const unsigned long long q2 = (unsigned long long)(Qv * Qv);
                     const size_t o = ((size_t)w * T + t) * 32 + b;
