@@ -1,0 +1,78 @@
+"""Result tables from `<H>-obs.bin` files, computed in chunks.
+
+Restates the estimators of the reference's analyze-all.py (lines 29-88): drop
+the first half of the record series (thermalisation), then per temperature
+  chi_0  = [<q_0^2>]                       (disorder average of thermal means)
+  xi_L/L = sqrt(chi_0/chi_1 - 1) / (2 sin(pi/L)) / L,  chi_1 from q_1 (3 axes)
+  e, m   = [<e>], [<m>]  (thermal mean over measurements and both copies)
+with errors from the variance over disorder samples.  Output rows have the
+reference's 9 columns (beta, chi0, err, xi_L/L, err, e, err, m, err) in the
+same format.  Reads the file in chunks, so tables of multi-GB series fit in a
+few hundred MB of memory.
+
+  python spin-glass_b200/analysis.py <obs.bin> <L> <NDIS> <NREP> [SBMEAS] [out.dat]
+"""
+from __future__ import annotations
+
+import sys
+
+import numpy as np
+
+OBS_DT = np.dtype([("e", "f4", (2,)), ("m", "f4", (2,)), ("q_0", "f4"), ("q_1_r", "f4", (3,)),
+                   ("q_1_i", "f4", (3,))])
+
+
+def analyze(path: str, L: int, ndis: int, nrep: int, betas=None, chunk: int = 8) -> dict:
+    rec = ndis * nrep * OBS_DT.itemsize
+    size = np.memmap(path, dtype=np.uint8, mode="r").size
+    therm = size // 2
+    data = np.memmap(path, dtype=OBS_DT, mode="r", offset=therm)
+    data = data[: (data.size // (ndis * nrep)) * ndis * nrep].reshape(-1, ndis, nrep)
+    n = data.shape[0]
+    if n == 0:
+        raise ValueError("no records after the thermalisation half")
+    s_q0 = np.zeros((ndis, nrep))
+    s_qr = np.zeros((ndis, nrep, 3))
+    s_qi = np.zeros((ndis, nrep, 3))
+    s_e = np.zeros((ndis, nrep))
+    s_m = np.zeros((ndis, nrep))
+    for a in range(0, n, chunk):
+        d = np.asarray(data[a:a + chunk])
+        s_q0 += (d["q_0"].astype(np.float64) ** 2).sum(axis=0)
+        s_qr += (d["q_1_r"].astype(np.float64) ** 2).sum(axis=0)
+        s_qi += (d["q_1_i"].astype(np.float64) ** 2).sum(axis=0)
+        s_e += d["e"].astype(np.float64).sum(axis=(0, 3))
+        s_m += d["m"].astype(np.float64).sum(axis=(0, 3))
+    chi0 = s_q0 / n
+    chi0_aa, chi0_v = chi0.mean(axis=0), chi0.var(axis=0)
+    chi1r, chi1i = s_qr / n, s_qi / n
+    chi1_aa = (chi1r.mean(axis=0) + chi1i.mean(axis=0)).mean(axis=1)
+    chi1_v = (chi1r.var(axis=0) + chi1i.var(axis=0)).mean(axis=1)
+    chif = chi0_aa / chi1_aa
+    chif_v = chif ** 2 * (chi0_v / chi0_aa ** 2 + chi1_v / chi1_aa ** 2)
+    xi = np.sqrt(chif - 1) / (2 * np.sin(np.pi / L)) / L
+    xi_v = (xi / (2 * (chif - 1))) ** 2 * chif_v
+    e = s_e / (2 * n)
+    m = s_m / (2 * n)
+    if betas is None:
+        betas = np.logspace(1, -3, num=nrep, base=2.0)
+    return {"beta": np.asarray(betas), "chi0": chi0_aa, "chi0_err": np.sqrt(chi0_v / ndis),
+            "xi": xi, "xi_err": np.sqrt(xi_v / ndis), "e": e.mean(axis=0),
+            "e_err": np.sqrt(e.var(axis=0) / ndis), "m": m.mean(axis=0),
+            "m_err": np.sqrt(m.var(axis=0) / ndis), "n_meas": n}
+
+
+def write_table(res: dict, path: str, sweeps_per_meas: int = 1024) -> None:
+    with open(path, "w") as f:
+        f.write(f"# tot_MC_steps : {2 * res['n_meas'] * sweeps_per_meas:,}\n")
+        cols = ["beta", "chi0", "chi0_err", "xi", "xi_err", "e", "e_err", "m", "m_err"]
+        for r in range(len(res["beta"])):
+            f.write("".join(f"{res[c][r]:16.12f}" for c in cols) + "\n")
+
+
+if __name__ == "__main__":
+    obs, L, ndis, nrep = sys.argv[1], int(sys.argv[2]), int(sys.argv[3]), int(sys.argv[4])
+    sbmeas = int(sys.argv[5]) if len(sys.argv) > 5 else 1024
+    out = sys.argv[6] if len(sys.argv) > 6 else obs.replace("-obs.bin", "-res.dat")
+    write_table(analyze(obs, L, ndis, nrep), out, sbmeas)
+    print(out)

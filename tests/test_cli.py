@@ -66,6 +66,20 @@ def test_reference_analysis_reads_our_records_unchanged(orc, tmp_path):
     rows = np.array([[float(v) for v in ln.split()] for ln in res[1:]])
     assert rows.shape == (24, 9)
     np.testing.assert_allclose(rows[:, 0], np.logspace(1, -3, 24, base=2.0))
+    # the chunked restatement (spin-glass_b200/analysis.py) gives the same tables
+    # (it accumulates in float64 where analyze-all.py averages float32 arrays)
+    sys.path.insert(0, str(ROOT / "spin-glass_b200"))
+    import analysis
+    for L, H in [(12, 0.0), (16, 0.1875)]:
+        mine = tmp_path / f"mine-{L}-{H}.dat"
+        analysis.write_table(analysis.analyze(str(sim / f"{L:02d}" / f"{H:06.4f}-obs.bin"), L,
+                                              2048, 24, chunk=1), str(mine))
+        want = (sim / f"{L:02d}" / f"{H:06.4f}-res.dat").read_text().splitlines()
+        got = mine.read_text().splitlines()
+        assert got[0] == want[0]
+        np.testing.assert_allclose(np.array([[float(v) for v in ln.split()] for ln in got[1:]]),
+                                   np.array([[float(v) for v in ln.split()] for ln in want[1:]]),
+                                   rtol=1e-3, atol=1e-9)
 
 
 # ---------------------------------------------------------------- on the GPU
