@@ -312,6 +312,57 @@ def run_e2e(csg, torch, betas, seed, args) -> dict:
             "h2d": int(hs.nbytes + hb.nbytes), "d2h": int(d2h)}
 
 
+MIXED = [  # L, sample words, temperatures (batched, uneven sizes; 2 copies each)
+    (12, 16, 16), (14, 12, 20), (16, 8, 24)]
+
+
+def run_mixed(args) -> None:
+    """Batched engine on the mixed L=12/14/16 workload vs the plain engine
+    looping over the same lattices (one step = 1024 sweeps of every member)."""
+    csg = _package()
+    members = [dict(L=l, n_words=w, n_copies=NCOPY,
+                    betas=1.0 / (T_MIN * (T_MAX / T_MIN) ** (np.arange(t) / (t - 1))),
+                    seed=SEED + l, sweeps_per_swap=args.swap_every,
+                    sweeps_per_meas=args.measure_every) for l, w, t in MIXED]
+    per_sweep = sum(l ** 3 * w * 32 * NCOPY * t for l, w, t in MIXED)
+    with csg.Batch(members) as b:
+        for e in b.members:
+            e.init_lattice()
+        chosen = b.tune(64)
+        for k in range(args.warmup):
+            b.run(SWEEPS_PER_STEP)
+        with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+            t0 = time.perf_counter()
+            for k in range(args.steps):
+                b.run(SWEEPS_PER_STEP)
+            batched_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        for k in range(args.steps):
+            b.run_sequential(SWEEPS_PER_STEP)
+        plain_s = time.perf_counter() - t0
+        b.set_plan([0] * len(members))  # the plain engine with its own per-member plans
+        t0 = time.perf_counter()
+        for k in range(args.steps):
+            b.run_sequential(SWEEPS_PER_STEP)
+        plain_auto_s = time.perf_counter() - t0
+    att = args.steps * SWEEPS_PER_STEP * per_sweep
+    line = {"metric": METRIC, "value": att / (batched_s * 1e9), "unit": METRIC, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": batched_s * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": "batched, uneven sizes (L=12 x512, L=14 x384, L=16 x256 "
+                                   "samples; 16/20/24 temperatures in T=[0.2,2]; 2 copies)",
+                       "sweeps_per_step": SWEEPS_PER_STEP, "swap_every": args.swap_every,
+                       "measure_every": args.measure_every,
+                       "timing": "host clock around synchronous graph launches",
+                       "quads_per_cta_tuned": [int(q) for q in chosen]},
+            "plain_value": att / (plain_auto_s * 1e9),
+            "plain_value_tuned_plans": att / (plain_s * 1e9),
+            "batched_over_plain": plain_auto_s / batched_s,
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -322,6 +373,7 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--swap-every", type=int, default=1, help="sweeps per exchange round (0: none)")
     ap.add_argument("--measure-every", type=int, default=1, help="sweeps per measurement (0: none)")
+    ap.add_argument("--workload", choices=["production", "mixed"], default="production")
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the end-to-end leg (profiling runs)")
     args = ap.parse_args()
@@ -330,6 +382,10 @@ def main() -> None:
     dist = None
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload == "mixed":
+        if rank == 0:
+            run_mixed(args)
         return
     if world > 1:
         import datetime

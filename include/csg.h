@@ -211,6 +211,37 @@ int csg_set_plan_override(const csg_plan* plan);
 int csg_obs_records_noalloc(const csg_config* cfg, const uint32_t* spins, const uint32_t* bonds,
                             float* rec, size_t n_floats, void* stream);
 
+/* ---- Batched engine -------------------------------------------------------
+ * No counterpart in the reference, which compiles one lattice size into its
+ * binary (eamsim.cuh:13) and runs one simulation per process.  A batch holds
+ * several simulations (any mix of L, sample counts, ladders, schedules), each
+ * a full engine, and advances all of them with one launch of a captured CUDA
+ * graph whose parallel branches are the members' cluster-resident kernels.
+ * Every member keeps its own Philox counters: its results are bit-identical
+ * to running it alone. */
+typedef struct csg_batch csg_batch;
+
+int csg_batch_create(const csg_config* cfgs, int32_t n, csg_batch** out);
+int csg_batch_destroy(csg_batch* b);
+
+/* Borrowed handle of member i (init / set / get state, observables, ...). */
+int csg_batch_engine(csg_batch* b, int32_t i, csg_engine** out);
+
+/* n_sweeps sweeps of every member, one graph launch (the graph is captured on
+ * first use for this n_sweeps and replayed afterwards). */
+int csg_batch_run(csg_batch* b, int64_t n_sweeps);
+
+/* The same work as the plain engine would do it: member after member. */
+int csg_batch_run_sequential(csg_batch* b, int64_t n_sweeps);
+
+/* Autotuner: chooses each member's quads per CTA (hence its cluster size) by
+ * timing the whole batch for probe_sweeps sweeps; states are restored after.
+ * chosen (may be NULL) receives the choice per member. */
+int csg_batch_tune(csg_batch* b, int64_t probe_sweeps, int32_t* chosen);
+
+/* Set each member's quads per CTA (0 = automatic). */
+int csg_batch_set_plan(csg_batch* b, const int32_t* quads_per_cta);
+
 #ifdef __cplusplus
 }
 #endif

@@ -96,6 +96,13 @@ def lib():
             "csg_init_device": [pcfg, vp, vp, vp],
             "csg_query_plan": [pcfg, C.POINTER(Plan)],
             "csg_set_plan_override": [C.POINTER(Plan)],
+            "csg_batch_create": [C.POINTER(Config), C.c_int32, C.POINTER(vp)],
+            "csg_batch_destroy": [vp],
+            "csg_batch_engine": [vp, C.c_int32, C.POINTER(vp)],
+            "csg_batch_run": [vp, i64],
+            "csg_batch_run_sequential": [vp, i64],
+            "csg_batch_tune": [vp, i64, vp],
+            "csg_batch_set_plan": [vp, vp],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -282,3 +289,76 @@ def reference_betas(T: int = 24) -> np.ndarray:
     """beta_r = 2 (2^(-4/(T-1)))^r stored as float32, as eamsim.cu:728-737."""
     ratio = 2.0 ** (-4.0 / (T - 1.0))
     return np.array([np.float32(ratio ** r * 2.0) for r in range(T)], dtype=np.float64)
+
+
+class _Member(Engine):
+    """A batch member: an Engine view whose handle the batch owns."""
+
+    def __init__(self, handle, cfg, betas, log_rounds):
+        self.cfg, self._betas = cfg, betas
+        d = cfg.dims
+        self.L, self.W, self.C, self.T = d.L, d.n_words, d.n_copies, d.n_temps
+        self.N = d.L ** 3
+        self._log_rounds = log_rounds
+        self._h = handle
+
+    def close(self) -> None:  # the batch destroys its members
+        self._h = None
+
+
+class Batch:
+    """Several simulations advanced together (csg_batch_* entry points).
+
+    members: list of dicts with the keyword arguments of Engine
+    (L, n_words, n_copies, betas, and optional H, seed, schedule...)."""
+
+    def __init__(self, members):
+        made = [make_config(m["L"], m["n_words"], m["n_copies"], m["betas"],
+                            **{k: v for k, v in m.items()
+                               if k not in ("L", "n_words", "n_copies", "betas")})
+                for m in members]
+        self._betas = [b for _, b in made]
+        arr = (Config * len(made))(*[c for c, _ in made])
+        self._cfgs = arr
+        h = C.c_void_p()
+        _check(lib().csg_batch_create(arr, len(made), C.byref(h)))
+        self._h = h
+        self.members = []
+        for i, m in enumerate(members):
+            eh = C.c_void_p()
+            _check(lib().csg_batch_engine(self._h, i, C.byref(eh)))
+            self.members.append(_Member(eh, arr[i], self._betas[i], m.get("swap_log_rounds", 0)))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            for m in self.members:
+                m._h = None
+            lib().csg_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def run(self, n_sweeps: int) -> None:
+        _check(lib().csg_batch_run(self._h, n_sweeps))
+
+    def run_sequential(self, n_sweeps: int) -> None:
+        _check(lib().csg_batch_run_sequential(self._h, n_sweeps))
+
+    def tune(self, probe_sweeps: int = 64):
+        out = np.zeros(len(self.members), np.int32)
+        _check(lib().csg_batch_tune(self._h, probe_sweeps, _p(out)))
+        return out
+
+    def set_plan(self, quads_per_cta) -> None:
+        q = np.ascontiguousarray(quads_per_cta, np.int32)
+        _check(lib().csg_batch_set_plan(self._h, _p(q)))

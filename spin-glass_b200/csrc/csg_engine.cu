@@ -179,7 +179,7 @@ void fill_launch(cudaLaunchConfig_t& lc, cudaLaunchAttribute* attr, int W, const
 // cluster.  The score is the number of quads the busiest SM must sweep
 // (waves of co-resident clusters times the quads per SM in a wave); ties go
 // to the smaller cluster (fewer cross-CTA exchanges).
-int make_plan(const csg_config& cfg, bool gen, Plan& out) {
+int make_plan(const csg_config& cfg, bool gen, Plan& out, int forced_qc = 0) {
     const int L = cfg.dims.L, W = cfg.dims.n_words;
     const int G = cfg.dims.n_copies * cfg.dims.n_temps / 4;
     const int tpq = csg::tpq_for(L);
@@ -188,8 +188,8 @@ int make_plan(const csg_config& cfg, bool gen, Plan& out) {
     if (!fn) return fail(CSG_ERR_UNSUPPORTED, "no kernel for L");
     {
         std::lock_guard<std::mutex> lk(g_plan_mu);
-        if (g_override.quads_per_cta > 0) {
-            const int Qc = g_override.quads_per_cta;
+        if (forced_qc > 0 || g_override.quads_per_cta > 0) {
+            const int Qc = forced_qc > 0 ? forced_qc : g_override.quads_per_cta;
             if (G % Qc != 0) return fail(CSG_ERR_ARG, "plan override does not divide the quads");
             out.Qc = Qc;
             out.K = G / Qc;
@@ -262,12 +262,17 @@ int fill_params(const csg_config& cfg, csg::PtParams& P, bool& gen) {
 constexpr int64_t kSweepsPerLaunch = 1024;
 
 int run_device(const csg_config& cfg, uint32_t* spins, const uint32_t* bonds,
-               const csg_device_obs* obs, int64_t sweep0, int64_t n_sweeps, cudaStream_t st) {
+               const csg_device_obs* obs, int64_t sweep0, int64_t n_sweeps, cudaStream_t st,
+               int forced_qc = 0, long long* sweep_dev = nullptr, const Plan* plan_in = nullptr) {
     csg::PtParams P;
     bool gen = false;
     fill_params(cfg, P, gen);
     Plan pl;
-    if (int rc = make_plan(cfg, gen, pl)) return rc;
+    if (plan_in)
+        pl = *plan_in;  // planned before a stream capture
+    else if (int rc = make_plan(cfg, gen, pl, forced_qc))
+        return rc;
+    P.sweep_dev = sweep_dev;
     KernelFn fn = select_kernel(cfg.dims.L, gen);
     P.spins = spins;
     P.bonds = bonds;
@@ -296,6 +301,10 @@ int run_device(const csg_config& cfg, uint32_t* spins, const uint32_t* bonds,
         cudaLaunchAttribute attr[1];
         fill_launch(lc, attr, cfg.dims.n_words, pl, st);
         CSG_CUDA(cudaLaunchKernelEx(&lc, fn, P));
+        if (sweep_dev) {
+            csg::advance_counter<<<1, 1, 0, st>>>(sweep_dev, (long long)P.n_sweeps);
+            CSG_CUDA(cudaGetLastError());
+        }
     }
     return CSG_OK;
 }
@@ -321,6 +330,7 @@ struct csg_engine {
     uint32_t* swap_log = nullptr;
     uint64_t* boundary = nullptr;
     int64_t sweep = 0, n_meas = 0, swap_rounds = 0, swap_round0 = 0;
+    int qc = 0;  // quads per CTA chosen by a batch's tuner (0: automatic plan)
 };
 
 namespace {
@@ -515,7 +525,7 @@ int csg_run(csg_engine* e, int64_t n_sweeps) {
     if (n_sweeps < 0) return fail(CSG_ERR_ARG, "negative sweep count");
     if (n_sweeps == 0) return CSG_OK;
     const csg_device_obs o = device_obs(e);
-    if (int rc = run_device(e->cfg, e->spins, e->bonds, &o, e->sweep, n_sweeps, e->stream))
+    if (int rc = run_device(e->cfg, e->spins, e->bonds, &o, e->sweep, n_sweeps, e->stream, e->qc))
         return rc;
     const csg_schedule& sc = e->cfg.sched;
     e->swap_rounds += count_events(e->sweep, n_sweeps, sc.sweeps_per_swap, 0);
@@ -770,6 +780,280 @@ int csg_load_checkpoint(csg_engine* e, const uint32_t* ref, size_t n_words, int6
                         for (int t = 0; t < T; ++t) sp[spin_at(d, w, c, t, si)] = sv[c][t];
                 }
     return csg_set_state(e, sp.data(), sp.size(), bd.data(), bd.size(), sweep);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched engine: several simulations (any mix of L, samples, ladders) run as
+// parallel branches of one captured CUDA graph, so that their clusters share
+// the SMs that any single one leaves idle.  Each member keeps its own Philox
+// counters, so its results do not depend on the batch it runs in.
+// ---------------------------------------------------------------------------
+struct csg_batch {
+    std::vector<csg_engine*> eng;
+    cudaStream_t main = nullptr;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
+    long long* counters = nullptr;  // device sweep counter per member
+    std::vector<std::pair<int64_t, cudaGraphExec_t>> graphs;
+};
+
+namespace {
+
+void drop_graphs(csg_batch* b) {
+    for (auto& g : b->graphs) cudaGraphExecDestroy(g.second);
+    b->graphs.clear();
+}
+
+int plan_member(csg_engine* e, Plan& pl) {
+    csg::PtParams P;
+    bool gen = false;
+    fill_params(e->cfg, P, gen);
+    return make_plan(e->cfg, gen, pl, e->qc);
+}
+
+int capture(csg_batch* b, int64_t n_sweeps, bool with_obs, cudaGraphExec_t* out) {
+    std::vector<Plan> plans(b->eng.size());
+    for (size_t i = 0; i < b->eng.size(); ++i)
+        if (int rc = plan_member(b->eng[i], plans[i])) return rc;
+    CSG_CUDA(cudaStreamBeginCapture(b->main, cudaStreamCaptureModeThreadLocal));
+    int rc = CSG_OK;
+    cudaError_t ce = cudaEventRecord(b->fork, b->main);
+    for (size_t i = 0; i < b->eng.size() && rc == CSG_OK && ce == cudaSuccess; ++i) {
+        csg_engine* e = b->eng[i];
+        ce = cudaStreamWaitEvent(e->stream, b->fork, 0);
+        if (ce != cudaSuccess) break;
+        const csg_device_obs o = device_obs(e);
+        rc = run_device(e->cfg, e->spins, e->bonds, with_obs ? &o : nullptr, 0, n_sweeps, e->stream,
+                        0, b->counters + i, &plans[i]);
+        if (rc == CSG_OK) ce = cudaEventRecord(b->join[i], e->stream);
+        if (ce == cudaSuccess) ce = cudaStreamWaitEvent(b->main, b->join[i], 0);
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce2 = cudaStreamEndCapture(b->main, &g);
+    if (rc != CSG_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (ce != cudaSuccess || ce2 != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return fail(CSG_ERR_CUDA, std::string("graph capture: ") +
+                                      cudaGetErrorString(ce != cudaSuccess ? ce : ce2));
+    }
+    const cudaError_t ce3 = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (ce3 != cudaSuccess)
+        return fail(CSG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce3));
+    return CSG_OK;
+}
+
+// Launch the batch graph for n sweeps from the members' host sweep counters.
+int launch_batch(csg_batch* b, int64_t n_sweeps, bool with_obs) {
+    for (csg_engine* e : b->eng) CSG_CUDA(cudaStreamSynchronize(e->stream));
+    cudaGraphExec_t exec = nullptr;
+    if (with_obs)
+        for (auto& g : b->graphs)
+            if (g.first == n_sweeps) exec = g.second;
+    if (!exec) {
+        if (int rc = capture(b, n_sweeps, with_obs, &exec)) return rc;
+        if (with_obs) b->graphs.push_back({n_sweeps, exec});
+    }
+    std::vector<long long> start(b->eng.size());
+    for (size_t i = 0; i < b->eng.size(); ++i) start[i] = b->eng[i]->sweep;
+    CSG_CUDA(cudaMemcpyAsync(b->counters, start.data(), start.size() * sizeof(long long),
+                             cudaMemcpyHostToDevice, b->main));
+    CSG_CUDA(cudaGraphLaunch(exec, b->main));
+    if (!with_obs) {
+        CSG_CUDA(cudaStreamSynchronize(b->main));
+        cudaGraphExecDestroy(exec);
+    }
+    return CSG_OK;
+}
+
+void account(csg_engine* e, int64_t n) {
+    const csg_schedule& sc = e->cfg.sched;
+    e->swap_rounds += count_events(e->sweep, n, sc.sweeps_per_swap, 0);
+    e->n_meas += count_events(e->sweep, n, sc.sweeps_per_meas, sc.meas_start);
+    e->sweep += n;
+}
+
+}  // namespace
+
+extern "C" {
+
+int csg_batch_create(const csg_config* cfgs, int32_t n, csg_batch** out) {
+    if (!out || !cfgs || n < 1) return fail(CSG_ERR_ARG, "bad batch arguments");
+    *out = nullptr;
+    csg_batch* b = new (std::nothrow) csg_batch();
+    if (!b) return fail(CSG_ERR_NOMEM, "host allocation failed");
+    int rc = CSG_OK;
+    for (int i = 0; i < n && rc == CSG_OK; ++i) {
+        csg_engine* e = nullptr;
+        rc = csg_engine_create(&cfgs[i], &e);
+        if (rc == CSG_OK) b->eng.push_back(e);
+    }
+    if (rc == CSG_OK && cudaStreamCreateWithFlags(&b->main, cudaStreamNonBlocking) != cudaSuccess)
+        rc = fail(CSG_ERR_CUDA, "cudaStreamCreate failed");
+    if (rc == CSG_OK && cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess)
+        rc = fail(CSG_ERR_CUDA, "cudaEventCreate failed");
+    for (int i = 0; i < n && rc == CSG_OK; ++i) {
+        cudaEvent_t ev;
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
+            rc = fail(CSG_ERR_CUDA, "cudaEventCreate failed");
+        else
+            b->join.push_back(ev);
+    }
+    if (rc == CSG_OK) rc = dalloc(&b->counters, (size_t)n);
+    if (rc != CSG_OK) {
+        const std::string msg = g_err;
+        csg_batch_destroy(b);
+        g_err = msg;
+        return rc;
+    }
+    *out = b;
+    return CSG_OK;
+}
+
+int csg_batch_destroy(csg_batch* b) {
+    if (!b) return CSG_OK;
+    if (b->main) cudaStreamSynchronize(b->main);
+    drop_graphs(b);
+    for (csg_engine* e : b->eng) csg_engine_destroy(e);
+    for (cudaEvent_t ev : b->join) cudaEventDestroy(ev);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->main) cudaStreamDestroy(b->main);
+    if (b->counters) cudaFree(b->counters);
+    delete b;
+    return CSG_OK;
+}
+
+int csg_batch_engine(csg_batch* b, int32_t i, csg_engine** out) {
+    if (!b || !out || i < 0 || i >= (int32_t)b->eng.size()) return fail(CSG_ERR_ARG, "bad member index");
+    *out = b->eng[i];
+    return CSG_OK;
+}
+
+int csg_batch_run(csg_batch* b, int64_t n_sweeps) {
+    if (!b || n_sweeps < 0) return fail(CSG_ERR_ARG, "bad batch run arguments");
+    if (n_sweeps == 0) return CSG_OK;
+    if (int rc = launch_batch(b, n_sweeps, true)) return rc;
+    CSG_CUDA(cudaStreamSynchronize(b->main));
+    for (csg_engine* e : b->eng) account(e, n_sweeps);
+    return CSG_OK;
+}
+
+int csg_batch_run_sequential(csg_batch* b, int64_t n_sweeps) {
+    if (!b || n_sweeps < 0) return fail(CSG_ERR_ARG, "bad batch run arguments");
+    for (csg_engine* e : b->eng) CSG_CUDA(cudaStreamSynchronize(e->stream));
+    for (csg_engine* e : b->eng) {
+        const csg_device_obs o = device_obs(e);
+        if (int rc = run_device(e->cfg, e->spins, e->bonds, &o, e->sweep, n_sweeps, b->main, e->qc))
+            return rc;
+        account(e, n_sweeps);
+    }
+    CSG_CUDA(cudaStreamSynchronize(b->main));
+    return CSG_OK;
+}
+
+int csg_batch_set_plan(csg_batch* b, const int32_t* quads_per_cta) {
+    if (!b || !quads_per_cta) return fail(CSG_ERR_ARG, "null argument");
+    for (size_t i = 0; i < b->eng.size(); ++i) {
+        const csg_dims& d = b->eng[i]->cfg.dims;
+        const int G = d.n_copies * d.n_temps / 4;
+        if (quads_per_cta[i] < 0 || (quads_per_cta[i] > 0 && G % quads_per_cta[i]))
+            return fail(CSG_ERR_ARG, "quads_per_cta must divide n_copies*n_temps/4");
+    }
+    for (size_t i = 0; i < b->eng.size(); ++i) b->eng[i]->qc = quads_per_cta[i];
+    drop_graphs(b);
+    return CSG_OK;
+}
+
+// Autotuner: coordinate descent over each member's quads per CTA, timing the
+// whole batch graph for probe_sweeps sweeps (best of two) with every other
+// member fixed; two passes.  The members' spins are saved before and restored
+// after, and the probes accumulate no observables, so tuning leaves the
+// simulations exactly as they were.
+int csg_batch_tune(csg_batch* b, int64_t probe_sweeps, int32_t* chosen) {
+    if (!b || probe_sweeps < 1) return fail(CSG_ERR_ARG, "bad tune arguments");
+    const size_t n = b->eng.size();
+    std::vector<uint32_t*> saved(n, nullptr);
+    int rc = CSG_OK;
+    for (size_t i = 0; i < n && rc == CSG_OK; ++i) {
+        rc = dalloc(&saved[i], b->eng[i]->n_spins);
+        if (rc == CSG_OK)
+            if (cudaMemcpyAsync(saved[i], b->eng[i]->spins, b->eng[i]->n_spins * 4,
+                                cudaMemcpyDeviceToDevice, b->eng[i]->stream) != cudaSuccess)
+                rc = fail(CSG_ERR_CUDA, "snapshot copy failed");
+    }
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    if (rc == CSG_OK && (cudaEventCreate(&t0) != cudaSuccess || cudaEventCreate(&t1) != cudaSuccess))
+        rc = fail(CSG_ERR_CUDA, "cudaEventCreate failed");
+    auto time_batch = [&](float& ms_out) -> int {
+        cudaGraphExec_t exec = nullptr;
+        if (int r = capture(b, probe_sweeps, false, &exec)) return r;
+        float best = 1e30f;
+        for (int rep = 0; rep < 3; ++rep) {  // first launch warms up
+            std::vector<long long> start(n, 0);
+            CSG_CUDA(cudaMemcpyAsync(b->counters, start.data(), n * sizeof(long long),
+                                     cudaMemcpyHostToDevice, b->main));
+            CSG_CUDA(cudaEventRecord(t0, b->main));
+            CSG_CUDA(cudaGraphLaunch(exec, b->main));
+            CSG_CUDA(cudaEventRecord(t1, b->main));
+            CSG_CUDA(cudaEventSynchronize(t1));
+            float ms = 0.f;
+            CSG_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+            if (rep > 0 && ms < best) best = ms;
+        }
+        cudaGraphExecDestroy(exec);
+        ms_out = best;
+        return CSG_OK;
+    };
+    for (size_t i = 0; i < n && rc == CSG_OK; ++i) {
+        Plan pl;
+        rc = plan_member(b->eng[i], pl);  // start from the per-member plan
+        if (rc == CSG_OK) b->eng[i]->qc = pl.Qc;
+    }
+    for (int pass = 0; pass < 2 && rc == CSG_OK; ++pass)
+        for (size_t i = 0; i < n && rc == CSG_OK; ++i) {
+            csg_engine* e = b->eng[i];
+            const int G = e->cfg.dims.n_copies * e->cfg.dims.n_temps / 4;
+            const bool gen = e->cfg.H != 0.0;
+            const bool has_m = gen || (e->cfg.flags & CSG_MEASURE_M);
+            int best_qc = e->qc;
+            float best_ms = 1e30f;
+            for (int qc = 1; qc <= G && rc == CSG_OK; ++qc) {
+                if (G % qc || G / qc > 16 || smem_for(e->cfg.dims.L, qc, has_m, gen) > kMaxSmem ||
+                    qc * csg::tpq_for(e->cfg.dims.L) > csg::kMaxThreads)
+                    continue;
+                e->qc = qc;
+                float ms = 0.f;
+                const int r = time_batch(ms);
+                if (r != CSG_OK) {  // e.g. a cluster shape the device cannot place
+                    cudaGetLastError();
+                    continue;
+                }
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best_qc = qc;
+                }
+            }
+            e->qc = best_qc;
+        }
+    for (size_t i = 0; i < n; ++i) {
+        if (saved[i]) {
+            if (rc == CSG_OK &&
+                cudaMemcpy(b->eng[i]->spins, saved[i], b->eng[i]->n_spins * 4,
+                           cudaMemcpyDeviceToDevice) != cudaSuccess)
+                rc = fail(CSG_ERR_CUDA, "restore copy failed");
+            cudaFree(saved[i]);
+        }
+        if (chosen) chosen[i] = b->eng[i]->qc;
+    }
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
+    drop_graphs(b);
+    return rc;
 }
 
 }  // extern "C"

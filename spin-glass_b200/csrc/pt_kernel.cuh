@@ -64,6 +64,7 @@ struct PtParams {
     int W, C, T, Q;
     int K, Qc;
     long long sweep0;
+    const long long* sweep_dev;  // if set, added to sweep0 (lets a captured graph advance)
     int n_sweeps;
     int sps, spm;
     long long meas_start;
@@ -322,8 +323,9 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
     const uint32_t* thrq = sThr + (size_t)j * 4 * 14;
     const uint8_t* ucq = sUcut + (size_t)j * 4 * 2;
 
+    const long long sweep_base = P.sweep0 + (P.sweep_dev ? *P.sweep_dev : 0ll);
     for (int it = 0; it < P.n_sweeps; ++it) {
-        const long long s = P.sweep0 + it;
+        const long long s = sweep_base + it;
         const bool do_swap = P.sps > 0 && ((s + 1) % P.sps) == 0;
         const bool do_meas = P.spm > 0 && ((s + 1) % P.spm) == 0 && s >= P.meas_start;
         const bool need_E = do_swap || do_meas;
@@ -692,5 +694,8 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
     }
     cluster.sync();  // no CTA leaves while a peer may still read its shared memory
 }
+
+// Advances a device-resident sweep counter after a launch of a captured graph.
+__global__ void advance_counter(long long* counter, long long n) { *counter += n; }
 
 }  // namespace csg
