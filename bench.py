@@ -8,8 +8,9 @@ one section of 1024 sweeps = one kernel launch.  Synthetic, seeded disorder.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Prints one JSON line (rank 0).  With torchrun, every rank runs its own
-independent set of 1024 samples (weak scaling, no collective on the data path).
+Prints one JSON line (rank 0).  With torchrun, the ranks share one simulation
+of N x 1024 samples, 1024 per rank (sample words sharded with word0; weak
+scaling, no collective on the data path).
 """
 from __future__ import annotations
 
@@ -199,10 +200,10 @@ def run_ours(args, rank: int, world: int, dist) -> None:
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    seed = SEED + rank
+    seed = SEED  # one simulation of world x 1024 samples, sharded by sample word
     betas = 1.0 / (T_MIN * (T_MAX / T_MIN) ** (np.arange(T) / (T - 1)))
     cfg, _keep = csg.make_config(L, W, NCOPY, betas, seed=seed, sweeps_per_swap=args.swap_every,
-                                 sweeps_per_meas=args.measure_every, meas_start=0)
+                                 sweeps_per_meas=args.measure_every, meas_start=0, word0=rank * W)
     N = L ** 3
     spins = torch.empty(W * NCOPY * T * N, dtype=torch.int32, device=dev)
     bonds = torch.empty(W * 3 * N, dtype=torch.int32, device=dev)
@@ -250,7 +251,7 @@ def run_ours(args, rank: int, world: int, dist) -> None:
 
     # ---- end to end through the engine API: host state in, observables out ----
     e2e = ({"value": None, "seconds": 0.0, "attempts": 0, "h2d": 0, "d2h": 0}
-           if args.no_e2e else run_e2e(csg, torch, betas, seed, args))
+           if args.no_e2e else run_e2e(csg, torch, betas, seed, args, word0=rank * W))
     if dist is not None and not args.no_e2e:
         t = torch.tensor([e2e["seconds"]], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -281,14 +282,14 @@ def run_ours(args, rank: int, world: int, dist) -> None:
     print(json.dumps(line), flush=True)
 
 
-def run_e2e(csg, torch, betas, seed, args) -> dict:
+def run_e2e(csg, torch, betas, seed, args, word0: int = 0) -> dict:
     """csg_set_state (pinned host -> device), csg_run (one section),
     csg_get_observables (device -> host) per step, wall-clock timed."""
     N = L ** 3
     hs = torch.empty(W * NCOPY * T * N, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
     hb = torch.empty(W * 3 * N, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
     with csg.Engine(L, W, NCOPY, betas, seed=seed, sweeps_per_swap=args.swap_every,
-                    sweeps_per_meas=args.measure_every) as eng:
+                    sweeps_per_meas=args.measure_every, word0=word0) as eng:
         eng.init_lattice()
         s, b, _ = eng.get_state()
         hs[:] = s.ravel()

@@ -65,6 +65,9 @@ typedef struct csg_config {
     const double* betas;     /* n_temps inverse temperatures (host); exchanges pair t, t+1 */
     int32_t flags;           /* CSG_MEASURE_M */
     int32_t swap_log_rounds; /* keep accepted-exchange masks of this many rounds (tests) */
+    int32_t word0;           /* global index of the first sample word (Philox counter word
+                                2): a simulation split into shards of words with matching
+                                word0 reproduces the unsplit run bit for bit */
 } csg_config;
 
 /* Accumulated observables (host arrays; any pointer may be NULL).

@@ -192,8 +192,8 @@ int orc_thresholds(int32_t T, const double* betas, double H, uint64_t* thr) {
 // samples (eamsim.cu:589-595 draws three bits per site per sample).  Spins:
 // one block per (word, copy, site, temperature quad), uniform random
 // (eamsim.cu:570-574).
-int orc_init(int32_t L, int32_t W, int32_t C, int32_t T, uint64_t seed, uint32_t* spins,
-             uint32_t* bonds) {
+int orc_init(int32_t L, int32_t W, int32_t C, int32_t T, uint64_t seed, int32_t word0,
+             uint32_t* spins, uint32_t* bonds) {
     if (!dims_ok(L, W, C, T) || !spins || !bonds) return 1;
     const Dims D(L, W, C, T);
     const Geo& g = D.g;
@@ -203,11 +203,12 @@ int orc_init(int32_t L, int32_t W, int32_t C, int32_t T, uint64_t seed, uint32_t
                 for (int x = 0; x < L; ++x) {
                     const int64_t i = g.site(x, y, z), si = g.slot(x, y, z);
                     uint32_t r[4];
-                    philox_ctr((uint32_t)i, 0u, (uint32_t)w, kTagBond, seed, r);
+                    const uint32_t wg = (uint32_t)(w + word0);
+                    philox_ctr((uint32_t)i, 0u, wg, kTagBond, seed, r);
                     for (int d = 0; d < 3; ++d) bonds[D.bond(w, d, si)] = r[d];
                     for (int c = 0; c < C; ++c)
                         for (int q = 0; q < D.Q; ++q) {
-                            philox_ctr((uint32_t)i, 0u, (uint32_t)w,
+                            philox_ctr((uint32_t)i, 0u, wg,
                                        kTagInit | ((uint32_t)c << 8) | (uint32_t)q, seed, r);
                             for (int k = 0; k < 4; ++k) spins[D.spin(w, c, 4 * q + k, si)] = r[k];
                         }
@@ -278,7 +279,8 @@ int orc_run(const orc_params* p, uint32_t* spins, const uint32_t* bonds, int64_t
                                         bonds[D.bond(w, 1, nb[2])], bonds[D.bond(w, 1, si)],
                                         bonds[D.bond(w, 2, nb[4])], bonds[D.bond(w, 2, si)]};
                                     uint32_t r[4];
-                                    philox_ctr((uint32_t)g.site(x, y, z), (uint32_t)s, (uint32_t)w,
+                                    philox_ctr((uint32_t)g.site(x, y, z), (uint32_t)s,
+                                               (uint32_t)(w + p->word0),
                                                kTagSweep | ((uint32_t)c << 8) | (uint32_t)q, p->seed,
                                                r);
                                     for (int k = 0; k < 4; ++k) {
@@ -328,7 +330,7 @@ int orc_run(const orc_params* p, uint32_t* spins, const uint32_t* bonds, int64_t
                         uint32_t mask = 0;
                         for (int j = 0; j < 16; ++j) {
                             uint32_t r[4];
-                            philox_ctr((uint32_t)j, (uint32_t)s, (uint32_t)w,
+                            philox_ctr((uint32_t)j, (uint32_t)s, (uint32_t)(w + p->word0),
                                        kTagSwap | ((uint32_t)c << 8) | (uint32_t)t, p->seed, r);
                             for (int h = 0; h < 2; ++h) {
                                 const int b = 2 * j + h;

@@ -44,6 +44,7 @@ typedef struct orc_params {
     const double* betas;       /* [T] */
     const uint64_t* thr;       /* [T][2][7] from orc_thresholds */
     int32_t n_threads;         /* OpenMP threads, 0 = runtime default */
+    int32_t word0;             /* global index of word 0 (Philox counter word 2) */
 } orc_params;
 
 typedef struct orc_obs {
@@ -72,7 +73,7 @@ void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t ou
 int orc_thresholds(int32_t T, const double* betas, double H, uint64_t* thr);
 
 /* Bonds and initial spins from the seed. */
-int orc_init(int32_t L, int32_t W, int32_t C, int32_t T, uint64_t seed,
+int orc_init(int32_t L, int32_t W, int32_t C, int32_t T, uint64_t seed, int32_t word0,
              uint32_t* spins, uint32_t* bonds);
 
 /* n_sweeps sweeps starting at global sweep index sweep0, with the exchange

@@ -37,6 +37,7 @@ class Params(C.Structure):
         ("betas", C.c_void_p),
         ("thr", C.c_void_p),
         ("n_threads", C.c_int32),
+        ("word0", C.c_int32),
     ]
 
 
@@ -63,7 +64,7 @@ def lib():
         L.orc_philox4x32_10.argtypes = [vp, vp, vp]
         L.orc_philox4x32_10.restype = None
         L.orc_thresholds.argtypes = [C.c_int32, vp, C.c_double, vp]
-        L.orc_init.argtypes = [C.c_int32] * 4 + [C.c_uint64, vp, vp]
+        L.orc_init.argtypes = [C.c_int32] * 4 + [C.c_uint64, C.c_int32, vp, vp]
         L.orc_run.argtypes = [C.POINTER(Params), vp, vp, C.c_int64, C.c_int64, C.POINTER(Obs)]
         L.orc_energies.argtypes = [C.c_int32] * 4 + [vp, vp, vp, vp]
         L.orc_overlaps.argtypes = [C.c_int32] * 3 + [vp, vp, vp]
@@ -102,11 +103,11 @@ def thresholds(betas, H: float) -> np.ndarray:
     return thr
 
 
-def init(L: int, W: int, C_: int, T: int, seed: int):
+def init(L: int, W: int, C_: int, T: int, seed: int, word0: int = 0):
     N = L ** 3
     spins = np.zeros((W, C_, T // 4, N, 4), np.uint32)
     bonds = np.zeros((W, 3, N), np.uint32)
-    _check(lib().orc_init(L, W, C_, T, seed, _p(spins), _p(bonds)), "init")
+    _check(lib().orc_init(L, W, C_, T, seed, word0, _p(spins), _p(bonds)), "init")
     return spins, bonds
 
 
@@ -155,7 +156,8 @@ class Observables:
 
 def run(spins: np.ndarray, bonds: np.ndarray, *, L: int, betas, H: float, seed: int,
         sweep0: int, n_sweeps: int, sweeps_per_swap: int = 1, sweeps_per_meas: int = 0,
-        meas_start: int = 0, obs: Observables | None = None, n_threads: int = 0) -> Observables:
+        meas_start: int = 0, obs: Observables | None = None, n_threads: int = 0,
+        word0: int = 0) -> Observables:
     W, C_, Q = spins.shape[:3]
     T = 4 * Q
     b = np.ascontiguousarray(betas, dtype=np.float64)
@@ -164,7 +166,8 @@ def run(spins: np.ndarray, bonds: np.ndarray, *, L: int, betas, H: float, seed: 
         obs = Observables(L, W, C_, T)
     p = Params(L=L, W=W, C=C_, T=T, sweeps_per_swap=sweeps_per_swap,
                sweeps_per_meas=sweeps_per_meas, meas_start=meas_start, H=float(H),
-               seed=seed, betas=_p(b).value, thr=_p(thr).value, n_threads=n_threads)
+               seed=seed, betas=_p(b).value, thr=_p(thr).value, n_threads=n_threads,
+               word0=word0)
     _check(lib().orc_run(C.byref(p), _p(spins), _p(bonds), sweep0, n_sweeps, C.byref(obs.c)),
            "run")
     return obs

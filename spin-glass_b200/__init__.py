@@ -37,7 +37,8 @@ class Schedule(C.Structure):
 
 class Config(C.Structure):
     _fields_ = [("dims", Dims), ("sched", Schedule), ("H", C.c_double), ("seed", C.c_uint64),
-                ("betas", C.c_void_p), ("flags", C.c_int32), ("swap_log_rounds", C.c_int32)]
+                ("betas", C.c_void_p), ("flags", C.c_int32), ("swap_log_rounds", C.c_int32),
+                ("word0", C.c_int32)]
 
 
 class ObservablesC(C.Structure):
@@ -128,13 +129,13 @@ def _p(a):
 
 def make_config(L: int, n_words: int, n_copies: int, betas, *, H: float = 0.0, seed: int = 1,
                 sweeps_per_swap: int = 1, sweeps_per_meas: int = 0, meas_start: int = 0,
-                flags: int = 0, swap_log_rounds: int = 0):
+                flags: int = 0, swap_log_rounds: int = 0, word0: int = 0):
     """Build a csg_config; returns (config, betas array that must stay alive)."""
     b = np.ascontiguousarray(betas, dtype=np.float64)
     cfg = Config(dims=Dims(L, n_words, n_copies, b.size),
                  sched=Schedule(sweeps_per_swap, sweeps_per_meas, meas_start),
                  H=float(H), seed=seed, betas=b.ctypes.data, flags=flags,
-                 swap_log_rounds=swap_log_rounds)
+                 swap_log_rounds=swap_log_rounds, word0=word0)
     return cfg, b
 
 

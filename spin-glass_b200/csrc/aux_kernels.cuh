@@ -14,7 +14,7 @@
 namespace csg {
 
 __global__ void init_kernel(uint32_t* spins, uint32_t* bonds, int L, int W, int C, int Q,
-                            uint32_t k0, uint32_t k1) {
+                            uint32_t k0, uint32_t k1, uint32_t word0) {
     const long N = (long)L * L * L;
     const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (long)W * N) return;
@@ -22,14 +22,15 @@ __global__ void init_kernel(uint32_t* spins, uint32_t* bonds, int L, int W, int 
     const int i = (int)(idx - (long)w * N);
     const int x = i % L, y = (i / L) % L, z = i / (L * L);
     const long slot = (long)((x + y + z) & 1) * (N / 2) + (long)(z * L + y) * (L / 2) + (x >> 1);
-    const u32x4 rb = philox4x32_10((uint32_t)i, 0u, (uint32_t)w, kTagBond, k0, k1);
+    const uint32_t wg = (uint32_t)w + word0;
+    const u32x4 rb = philox4x32_10((uint32_t)i, 0u, wg, kTagBond, k0, k1);
     bonds[((long)w * 3 + 0) * N + slot] = rb.v0;
     bonds[((long)w * 3 + 1) * N + slot] = rb.v1;
     bonds[((long)w * 3 + 2) * N + slot] = rb.v2;
     uint4* sp = reinterpret_cast<uint4*>(spins);
     for (int c = 0; c < C; ++c)
         for (int q = 0; q < Q; ++q) {
-            const u32x4 r = philox4x32_10((uint32_t)i, 0u, (uint32_t)w,
+            const u32x4 r = philox4x32_10((uint32_t)i, 0u, wg,
                                           kTagInit | ((uint32_t)c << 8) | (uint32_t)q, k0, k1);
             sp[(((long)w * C + c) * Q + q) * N + slot] = make_uint4(r.v0, r.v1, r.v2, r.v3);
         }

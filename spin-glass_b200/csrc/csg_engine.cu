@@ -60,6 +60,7 @@ int validate(const csg_config* cfg) {
         cfg->sched.meas_start < 0)
         return fail(CSG_ERR_ARG, "negative schedule entry");
     if (cfg->swap_log_rounds < 0) return fail(CSG_ERR_ARG, "negative swap_log_rounds");
+    if (cfg->word0 < 0) return fail(CSG_ERR_ARG, "negative word0");
     return CSG_OK;
 }
 
@@ -248,6 +249,7 @@ int fill_params(const csg_config& cfg, csg::PtParams& P, bool& gen) {
     P.H = cfg.H;
     P.k0 = (uint32_t)cfg.seed;
     P.k1 = (uint32_t)(cfg.seed >> 32);
+    P.word0 = (uint32_t)cfg.word0;
     P.W = cfg.dims.n_words;
     P.C = cfg.dims.n_copies;
     P.T = cfg.dims.n_temps;
@@ -480,7 +482,7 @@ int csg_init_device(const csg_config* cfg, uint32_t* spins, uint32_t* bonds, voi
     const int block = 256;
     csg::init_kernel<<<(unsigned)((total + block - 1) / block), block, 0, (cudaStream_t)stream>>>(
         spins, bonds, d.L, d.n_words, d.n_copies, d.n_temps / 4, (uint32_t)cfg->seed,
-        (uint32_t)(cfg->seed >> 32));
+        (uint32_t)(cfg->seed >> 32), (uint32_t)cfg->word0);
     CSG_CUDA(cudaGetLastError());
     return CSG_OK;
 }

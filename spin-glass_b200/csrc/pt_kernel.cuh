@@ -61,6 +61,7 @@ struct PtParams {
     unsigned long long* boundary;
     double H;
     uint32_t k0, k1;
+    uint32_t word0;  // global index of word 0 (Philox counter word 2)
     int W, C, T, Q;
     int K, Qc;
     long long sweep0;
@@ -320,6 +321,7 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
     uint4* Sq = S + (size_t)j * N;
     const uint32_t* Fw = P.bonds + (size_t)w * 3 * N;
     const uint32_t ctr3 = kTagSweep | ((uint32_t)c << 8) | (uint32_t)q;
+    const uint32_t wg = (uint32_t)w + P.word0;  // global sample word
     const uint32_t* thrq = sThr + (size_t)j * 4 * 14;
     const uint8_t* ucq = sUcut + (size_t)j * 4 * 2;
 
@@ -379,7 +381,7 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
                         const uint32_t f0 = __ldg(Fo + nxm), f1 = __ldg(Fc + n);
                         const uint32_t f2 = __ldg(Fo + N + nym), f3 = __ldg(Fc + N + n);
                         const uint32_t f4 = __ldg(Fo + 2 * N + nzm), f5 = __ldg(Fc + 2 * N + n);
-                        const u32x4 r = philox4x32_10((uint32_t)((z * L + y) * L + x), s32, (uint32_t)w,
+                        const u32x4 r = philox4x32_10((uint32_t)((z * L + y) * L + x), s32, wg,
                                                       ctr3, P.k0, P.k1);
                         const uint32_t rr[4] = {r.v0, r.v1, r.v2, r.v3};
                         uint32_t cw[4] = {cv.x, cv.y, cv.z, cv.w};
@@ -479,7 +481,7 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
             auto uniform_for = [&](int pi) {
                 const int gg = rank * Qc + (pi >> 1);
                 const int cc = gg / Q, t = 4 * (gg - cc * Q) + par + 2 * (pi & 1);
-                const u32x4 r = philox4x32_10((uint32_t)(lane >> 1), s32, (uint32_t)w,
+                const u32x4 r = philox4x32_10((uint32_t)(lane >> 1), s32, wg,
                                               kTagSwap | ((uint32_t)cc << 8) | (uint32_t)t,
                                               P.k0, P.k1);
                 const uint32_t lo = (lane & 1) ? r.v2 : r.v0;
