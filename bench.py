@@ -364,6 +364,63 @@ def run_mixed(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_serving(args) -> None:
+    """Poisson request stream through the continuous-batching server: each
+    request draws L in {8..16} (even), 32..1024 samples (multiples of 32),
+    16..32 temperatures (multiples of 4) geometric in T=[0.2,2], 4096..65536
+    sweeps (multiples of 1024), seeded +-J disorder; exchange every sweep."""
+    csg = _package()
+    rng = np.random.default_rng(args.serve_seed)
+    n_req = args.serve_requests
+    gaps = rng.exponential(1.0 / args.serve_rate, n_req)
+    arrivals = np.cumsum(gaps) - gaps[0]
+    reqs = []
+    for i in range(n_req):
+        L_ = int(rng.choice([8, 10, 12, 14, 16]))
+        w = int(rng.integers(1, 33))
+        t = int(rng.choice([16, 20, 24, 28, 32]))
+        sweeps = 1024 * int(rng.integers(4, 65))
+        betas = 1.0 / (T_MIN * (T_MAX / T_MIN) ** (np.arange(t) / (t - 1)))
+        reqs.append((arrivals[i], sweeps, dict(L=L_, n_words=w, n_copies=NCOPY, betas=betas,
+                                               seed=SEED + 7919 * i, sweeps_per_swap=1,
+                                               sweeps_per_meas=0)))
+    work = sum(r[1] * r[2]["L"] ** 3 * r[2]["n_words"] * 32 * NCOPY * len(r[2]["betas"])
+               for r in reqs)
+    budget = int(args.serve_budget_gb * 2 ** 30)
+    lat, t_done, nxt, ids = {}, {}, 0, {}
+    peak = 0
+    with csg.Server(budget, max_active=args.serve_slots, sweeps_per_launch=1024) as srv:
+        t0 = time.perf_counter()
+        while len(t_done) < n_req:
+            now = time.perf_counter() - t0
+            while nxt < n_req and reqs[nxt][0] <= now:
+                ids[srv.submit(reqs[nxt][1], **reqs[nxt][2])] = nxt
+                nxt += 1
+            done, na, nq = srv.poll()
+            peak = max(peak, na)
+            now = time.perf_counter() - t0
+            for d in done:
+                k = ids[d]
+                t_done[k] = now
+                lat[k] = now - reqs[k][0]
+                srv.result(d)
+            if not done:
+                time.sleep(0.0005)
+        makespan = time.perf_counter() - t0
+    lats = np.array([lat[k] for k in range(n_req)])
+    line = {"metric": "serving: " + METRIC + " with p50/p99 completion latency",
+            "value": work / (makespan * 1e9), "unit": METRIC, "n_gpus": 1,
+            "higher_is_better": True, "dtype": "u32", "data": "synthetic",
+            "latency_s": {"p50": float(np.percentile(lats, 50)),
+                          "p99": float(np.percentile(lats, 99)), "max": float(lats.max())},
+            "config": {"workload": "serving stream, Poisson arrivals",
+                       "rate_per_s": args.serve_rate, "requests": n_req,
+                       "memory_budget_GiB": args.serve_budget_gb, "max_active": args.serve_slots,
+                       "seed": args.serve_seed, "total_attempts": work,
+                       "makespan_s": makespan, "peak_active": peak}}
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -374,7 +431,13 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--swap-every", type=int, default=1, help="sweeps per exchange round (0: none)")
     ap.add_argument("--measure-every", type=int, default=1, help="sweeps per measurement (0: none)")
-    ap.add_argument("--workload", choices=["production", "mixed"], default="production")
+    ap.add_argument("--workload", choices=["production", "mixed", "serving"],
+                    default="production")
+    ap.add_argument("--serve-rate", type=float, default=2.0, help="requests per second")
+    ap.add_argument("--serve-requests", type=int, default=24)
+    ap.add_argument("--serve-budget-gb", type=float, default=16.0)
+    ap.add_argument("--serve-slots", type=int, default=32)
+    ap.add_argument("--serve-seed", type=int, default=5)
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the end-to-end leg (profiling runs)")
     args = ap.parse_args()
@@ -387,6 +450,10 @@ def main() -> None:
     if args.workload == "mixed":
         if rank == 0:
             run_mixed(args)
+        return
+    if args.workload == "serving":
+        if rank == 0:
+            run_serving(args)
         return
     if world > 1:
         import datetime

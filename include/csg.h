@@ -245,6 +245,35 @@ int csg_batch_tune(csg_batch* b, int64_t probe_sweeps, int32_t* chosen);
 /* Set each member's quads per CTA (0 = automatic). */
 int csg_batch_set_plan(csg_batch* b, const int32_t* quads_per_cta);
 
+/* ---- Serving: continuous batching -------------------------------------------
+ * No counterpart in the reference.  Requests (full simulation configurations
+ * plus a sweep count) are queued, admitted FIFO while a device-memory budget
+ * and an active-slot limit allow, initialised from their seeds on the GPU,
+ * and advanced section by section on their own streams, so that the kernels
+ * of different requests overlap on the device.  Each request keeps its own
+ * Philox counters: its result equals running it alone. */
+typedef struct csg_server csg_server;
+
+/* Device bytes an engine for this configuration allocates. */
+int csg_engine_footprint(const csg_config* cfg, size_t* bytes);
+
+int csg_server_create(size_t memory_budget_bytes, int32_t max_active, int32_t sweeps_per_launch,
+                      csg_server** out);
+int csg_server_destroy(csg_server* s);
+
+/* Queue a request; fails with CSG_ERR_NOMEM if it can never fit the budget. */
+int csg_server_submit(csg_server* s, const csg_config* cfg, int64_t n_sweeps, int64_t* id);
+
+/* Non-blocking scheduling pass (call it often): reports requests completed
+ * since the last pass (up to max_completed ids), active and queued counts. */
+int csg_server_poll(csg_server* s, int64_t* completed, int32_t max_completed,
+                    int32_t* n_completed, int32_t* n_active, int32_t* n_queued);
+
+/* Observables (and optionally the final spins) of a completed request;
+ * releases its memory.  Any output pointer may be NULL. */
+int csg_server_result(csg_server* s, int64_t id, csg_observables* obs, uint32_t* spins,
+                      size_t n_spins);
+
 #ifdef __cplusplus
 }
 #endif

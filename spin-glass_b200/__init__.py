@@ -104,6 +104,13 @@ def lib():
             "csg_batch_run_sequential": [vp, i64],
             "csg_batch_tune": [vp, i64, vp],
             "csg_batch_set_plan": [vp, vp],
+            "csg_engine_footprint": [C.POINTER(Config), C.POINTER(sz)],
+            "csg_server_create": [sz, C.c_int32, C.c_int32, C.POINTER(vp)],
+            "csg_server_destroy": [vp],
+            "csg_server_submit": [vp, C.POINTER(Config), i64, C.POINTER(i64)],
+            "csg_server_poll": [vp, vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                C.POINTER(C.c_int32)],
+            "csg_server_result": [vp, i64, C.POINTER(ObservablesC), vp, sz],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -363,3 +370,62 @@ class Batch:
     def set_plan(self, quads_per_cta) -> None:
         q = np.ascontiguousarray(quads_per_cta, np.int32)
         _check(lib().csg_batch_set_plan(self._h, _p(q)))
+
+
+def footprint(L: int, n_words: int, n_copies: int, betas, **kw) -> int:
+    """Device bytes an engine of this configuration allocates."""
+    cfg, _b = make_config(L, n_words, n_copies, betas, **kw)
+    out = C.c_size_t()
+    _check(lib().csg_engine_footprint(C.byref(cfg), C.byref(out)))
+    return int(out.value)
+
+
+class Server:
+    """Continuous-batching request server (csg_server_* entry points)."""
+
+    def __init__(self, memory_budget_bytes: int, max_active: int = 64,
+                 sweeps_per_launch: int = 1024):
+        h = C.c_void_p()
+        _check(lib().csg_server_create(memory_budget_bytes, max_active, sweeps_per_launch,
+                                       C.byref(h)))
+        self._h = h
+        self._req = {}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().csg_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def submit(self, n_sweeps: int, L: int, n_words: int, n_copies: int, betas, **kw) -> int:
+        cfg, b = make_config(L, n_words, n_copies, betas, **kw)
+        rid = C.c_int64()
+        _check(lib().csg_server_submit(self._h, C.byref(cfg), n_sweeps, C.byref(rid)))
+        self._req[rid.value] = (L, n_words, n_copies, b.size)
+        return rid.value
+
+    def poll(self, max_completed: int = 256):
+        ids = np.zeros(max_completed, np.int64)
+        nc, na, nq = C.c_int32(), C.c_int32(), C.c_int32()
+        _check(lib().csg_server_poll(self._h, _p(ids), max_completed, C.byref(nc), C.byref(na),
+                                     C.byref(nq)))
+        return [int(i) for i in ids[:min(nc.value, max_completed)]], na.value, nq.value
+
+    def result(self, rid: int, with_spins: bool = False):
+        L, W, C_, T = self._req.pop(rid)
+        o = Observables(L, W, C_, T)
+        spins = np.zeros((W, C_, T // 4, L ** 3, 4), np.uint32) if with_spins else None
+        _check(lib().csg_server_result(self._h, rid, C.byref(o.c), _p(spins),
+                                       spins.size if with_spins else 0))
+        return (o, spins) if with_spins else o

@@ -1,0 +1,68 @@
+"""Serving with continuous batching: requests of different L, sample counts and
+ladders admitted against a memory budget while others run; each result equals
+the same request run alone, bit for bit."""
+import time
+
+import numpy as np
+import pytest
+
+
+def request(i):
+    L = [8, 10, 12, 14, 16, 8][i % 6]
+    T = [8, 12, 16, 8, 12, 20][i % 6]
+    return dict(L=L, n_words=1 + i % 2, n_copies=2,
+                betas=1.0 / (0.3 * (2.0 / 0.3) ** (np.arange(T) / (T - 1))), seed=1000 + i,
+                sweeps_per_swap=1, sweeps_per_meas=2), 40 + 12 * i
+
+
+def test_footprint_and_validation(csg):
+    kw, _ = request(0)
+    fp = csg.footprint(**kw)
+    N = kw["L"] ** 3
+    assert fp > kw["n_words"] * 2 * len(kw["betas"]) * N * 4  # at least the spins
+    srv = csg.Server(fp * 3, max_active=4, sweeps_per_launch=16)
+    with pytest.raises(csg.CsgError):
+        srv.submit(10, **dict(kw, n_copies=3))
+    with pytest.raises(csg.CsgError, match="budget"):
+        big = dict(kw, n_words=64, L=24)
+        srv.submit(10, **big)
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_mixed_requests_equal_alone(csg):
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    reqs = [request(i) for i in range(6)]
+    budget = 3 * max(csg.footprint(**kw) for kw, _ in reqs)  # forces queueing
+    results, peak_active = {}, 0
+    with csg.Server(budget, max_active=8, sweeps_per_launch=16) as srv:
+        ids = {}
+        for k, (kw, n) in enumerate(reqs):
+            ids[srv.submit(n, **kw)] = k
+            if k % 2 == 1:  # arrivals while earlier requests run
+                done, na, nq = srv.poll()
+                peak_active = max(peak_active, na)
+                for d in done:
+                    results[ids[d]] = srv.result(d, with_spins=True)
+        deadline = time.time() + 120
+        while len(results) < len(reqs) and time.time() < deadline:
+            done, na, nq = srv.poll()
+            peak_active = max(peak_active, na)
+            for d in done:
+                results[ids[d]] = srv.result(d, with_spins=True)
+            time.sleep(0.001)
+    assert len(results) == len(reqs)
+    assert 1 < peak_active <= 3
+    for k, (kw, n) in enumerate(reqs):
+        with csg.Engine(**kw) as e:
+            e.init_lattice()
+            e.run(n)
+            s, _, _ = e.get_state()
+            o = e.observables()
+        o_srv, s_srv = results[k]
+        np.testing.assert_array_equal(s_srv, s)
+        np.testing.assert_array_equal(o_srv.e_sum, o.e_sum)
+        np.testing.assert_array_equal(o_srv.q2_sum, o.q2_sum)
+        assert o_srv.n_meas == o.n_meas
