@@ -55,8 +55,14 @@ def attempts_per_sweep() -> int:
     return L ** 3 * W * 32 * NCOPY * T
 
 
-def workload_config(n_gpus: int, swap_every: int = 1, measure_every: int = 1) -> dict:
-    return {"workload": "plain PT engine, production size", "L": L, "samples": 32 * W,
+def engine_flags(csg, args) -> int:
+    return csg.CSG_ENGINE_STREAM if getattr(args, "engine", "auto") == "stream" else 0
+
+
+def workload_config(n_gpus: int, swap_every: int = 1, measure_every: int = 1,
+                    engine: str = "auto") -> dict:
+    name = "plain PT engine, production size" + (" (streaming engine)" if engine == "stream" else "")
+    return {"workload": name, "L": L, "samples": 32 * W,
             "copies": NCOPY, "temperatures": T, "T_range": [T_MIN, T_MAX],
             "sweeps_per_step": SWEEPS_PER_STEP, "swap_every": swap_every,
             "measure_every": measure_every,
@@ -203,7 +209,8 @@ def run_ours(args, rank: int, world: int, dist) -> None:
     seed = SEED  # one simulation of world x 1024 samples, sharded by sample word
     betas = 1.0 / (T_MIN * (T_MAX / T_MIN) ** (np.arange(T) / (T - 1)))
     cfg, _keep = csg.make_config(L, W, NCOPY, betas, seed=seed, sweeps_per_swap=args.swap_every,
-                                 sweeps_per_meas=args.measure_every, meas_start=0, word0=rank * W)
+                                 sweeps_per_meas=args.measure_every, meas_start=0, word0=rank * W,
+                                 flags=engine_flags(csg, args))
     N = L ** 3
     spins = torch.empty(W * NCOPY * T * N, dtype=torch.int32, device=dev)
     bonds = torch.empty(W * 3 * N, dtype=torch.int32, device=dev)
@@ -267,14 +274,15 @@ def run_ours(args, rank: int, world: int, dist) -> None:
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic (seeded +-J disorder, uniform random initial spins)",
-            "config": workload_config(world, args.swap_every, args.measure_every),
+            "config": workload_config(world, args.swap_every, args.measure_every, args.engine),
             "roofline": {"bound": "int", "achieved": achieved / 1e12, "peak": peak["ops_per_s"] / 1e12,
                          "unit": "Tops/s (32-bit integer logic)",
                          "frac": achieved / peak["ops_per_s"], "traffic": profile_traffic(),
                          "ops_per_attempt": OPS_PER_WORD_UPDATE / 32, "peak_source": peak["source"]},
             "e2e": {"value": e2e["value"], "unit": METRIC,
                     "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]},
-            "gpu_launches": args.steps,
+            # resident kernel: one launch per 1024-sweep step; streaming engine: six per sweep
+            "gpu_launches": args.steps * (SWEEPS_PER_STEP * 6 if args.engine == "stream" else 1),
             "exchange_boundary_cases": boundary,
             "clocks": clk.summary()}
     if world == 1 and not args.no_cpu_baseline:
@@ -289,7 +297,8 @@ def run_e2e(csg, torch, betas, seed, args, word0: int = 0) -> dict:
     hs = torch.empty(W * NCOPY * T * N, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
     hb = torch.empty(W * 3 * N, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
     with csg.Engine(L, W, NCOPY, betas, seed=seed, sweeps_per_swap=args.swap_every,
-                    sweeps_per_meas=args.measure_every, word0=word0) as eng:
+                    sweeps_per_meas=args.measure_every, word0=word0,
+                    flags=engine_flags(csg, args)) as eng:
         eng.init_lattice()
         s, b, _ = eng.get_state()
         hs[:] = s.ravel()
@@ -364,6 +373,124 @@ def run_mixed(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+LARGE = [(32, 8, 32), (48, 8, 32)]  # L, sample words, temperatures (2 copies each)
+LARGE_T = (0.5, 2.0)
+LARGE_SWEEPS_PER_STEP = 256  # one step = 256 sweeps of a 4096-sweep run
+
+
+def measured_hbm_peak() -> dict:
+    f = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return {"gbs": float(json.loads(f.read_text())["hbm_gbs"]),
+                "source": "measured copy bandwidth (MEASURED_PEAKS.json)"}
+    except (OSError, ValueError, KeyError):
+        return {"gbs": 6650.0, "source": "fallback: earlier copy-bandwidth measurement on B200"}
+
+
+def run_large(args) -> None:
+    """Streaming engine at L=32 and L=48: 256 samples (8 words), 2 copies, 32
+    temperatures geometric in T=[0.5,2.0], exchange and measurement every sweep.
+
+    value = spin-flip attempts/ns at L=48 (the HBM-resident case; the L=32
+    state, 64 MiB of spins, stays in L2).  The roofline line is the colour
+    kernel's: its algorithmic bytes per launch (read and write its colour's
+    spin words, read the other colour's once, read the bonds once per word)
+    over its event-timed duration in a Metropolis-only run."""
+    import torch
+    csg = _package()
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device=dev)
+    peak = measured_hbm_peak()
+    by_L = {}
+    clk_summary = None
+    for (L_, W_, T_) in LARGE:
+        N = L_ ** 3
+        betas = 1.0 / (LARGE_T[0] * (LARGE_T[1] / LARGE_T[0]) ** (np.arange(T_) / (T_ - 1)))
+        cfg, _k1 = csg.make_config(L_, W_, NCOPY, betas, seed=SEED, sweeps_per_swap=1,
+                                   sweeps_per_meas=1)
+        metro, _k2 = csg.make_config(L_, W_, NCOPY, betas, seed=SEED, sweeps_per_swap=0,
+                                     sweeps_per_meas=0)
+        spins = torch.empty(W_ * NCOPY * T_ * N, dtype=torch.int32, device=dev)
+        bonds = torch.empty(W_ * 3 * N, dtype=torch.int32, device=dev)
+        z64 = lambda *s: torch.zeros(s, dtype=torch.int64, device=dev)
+        acc = {"e_sum": z64(W_, NCOPY, T_, 32), "q_sum": z64(W_, T_, 32),
+               "q2_sum": z64(W_, T_, 32), "q4_sum": z64(W_, T_, 32, 2),
+               "hist": torch.zeros((T_, N + 1), dtype=torch.int32, device=dev),
+               "e_last": torch.zeros((W_, NCOPY, T_, 32), dtype=torch.int32, device=dev),
+               "d_last": torch.zeros((W_, T_, 32), dtype=torch.int32, device=dev),
+               "boundary": z64(1)}
+        obs = csg.DeviceObs(**{k: v.data_ptr() for k, v in acc.items()})
+        csg.init_device(cfg, spins.data_ptr(), bonds.data_ptr(), stream.cuda_stream)
+        sweep = 0
+
+        def run(c, n, with_obs=True):
+            nonlocal sweep
+            csg.run_device(c, spins.data_ptr(), bonds.data_ptr(), obs if with_obs else None,
+                           sweep, n, stream.cuda_stream)
+            sweep += n
+
+        for _ in range(args.warmup):
+            run(cfg, LARGE_SWEEPS_PER_STEP)
+        torch.cuda.synchronize(dev)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]
+        with ClockSampler(0) as clk:
+            for k in range(args.steps):
+                flush.fill_(k)
+                ev[k][0].record(stream)
+                run(cfg, LARGE_SWEEPS_PER_STEP)
+                ev[k][1].record(stream)
+            torch.cuda.synchronize(dev)
+        t_ms = sum(a.elapsed_time(b) for a, b in ev)
+        if L_ == LARGE[-1][0]:
+            clk_summary = clk.summary()
+        # colour kernel alone: Metropolis-only sweeps (two colour launches each)
+        n_metro = 64
+        run(metro, 8, with_obs=False)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush.fill_(0)
+        a.record(stream)
+        run(metro, n_metro, with_obs=False)
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        colour_s = a.elapsed_time(b) * 1e-3 / (2 * n_metro)
+        quads = W_ * NCOPY * T_ // 4
+        colour_bytes = quads * (N // 2) * 16 * 3 + W_ * 3 * N * 4
+        per_sweep = N * 32 * W_ * NCOPY * T_
+        by_L[L_] = {"attempts_per_ns": args.steps * LARGE_SWEEPS_PER_STEP * per_sweep / (t_ms * 1e6),
+                    "ms_per_step": t_ms / args.steps,
+                    "us_per_sweep": t_ms * 1e3 / (args.steps * LARGE_SWEEPS_PER_STEP),
+                    "spin_bytes": W_ * NCOPY * T_ * N * 4,
+                    "metropolis_attempts_per_ns": per_sweep / (2 * colour_s * 1e9),
+                    "colour_kernel": {"us_per_launch": colour_s * 1e6,
+                                      "algorithmic_bytes_per_launch": colour_bytes,
+                                      "achieved_gbs": colour_bytes / colour_s / 1e9},
+                    "exchange_boundary_cases": int(acc["boundary"].item())}
+        del spins, bonds, acc
+    big = by_L[LARGE[-1][0]]
+    ck = big["colour_kernel"]
+    line = {"metric": METRIC, "value": big["attempts_per_ns"], "unit": METRIC, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": big["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded +-J disorder, uniform random initial spins)",
+            "config": {"workload": "large L, streaming engine (L=48; L=32 beside it)",
+                       "L": LARGE[-1][0], "samples": 32 * LARGE[-1][1], "copies": NCOPY,
+                       "temperatures": LARGE[-1][2], "T_range": list(LARGE_T),
+                       "sweeps_per_step": LARGE_SWEEPS_PER_STEP, "swap_every": 1,
+                       "measure_every": 1, "l2": "flushed between timed steps (256 MiB write); "
+                       "the L=48 state (227 MB) is larger than L2"},
+            "roofline": {"bound": "hbm", "achieved": ck["achieved_gbs"], "peak": peak["gbs"],
+                         "unit": "GB/s", "frac": ck["achieved_gbs"] / peak["gbs"],
+                         "traffic": None, "kernel": "stream_colour_kernel (Metropolis only)",
+                         "peak_source": peak["source"]},
+            "by_L": by_L,
+            # per sweep: 2 colour launches, exchange decisions, exchange, overlap, measurement
+            "gpu_launches": args.steps * LARGE_SWEEPS_PER_STEP * 6, "clocks": clk_summary}
+    print(json.dumps(line), flush=True)
+
+
 def run_serving(args) -> None:
     """Poisson request stream through the continuous-batching server: each
     request draws L in {8..16} (even), 32..1024 samples (multiples of 32),
@@ -431,8 +558,10 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--swap-every", type=int, default=1, help="sweeps per exchange round (0: none)")
     ap.add_argument("--measure-every", type=int, default=1, help="sweeps per measurement (0: none)")
-    ap.add_argument("--workload", choices=["production", "mixed", "serving"],
+    ap.add_argument("--workload", choices=["production", "mixed", "serving", "large"],
                     default="production")
+    ap.add_argument("--engine", choices=["auto", "stream"], default="auto",
+                    help="production workload: stream = force the streaming engine")
     ap.add_argument("--serve-rate", type=float, default=2.0, help="requests per second")
     ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--serve-budget-gb", type=float, default=16.0)
@@ -454,6 +583,10 @@ def main() -> None:
     if args.workload == "serving":
         if rank == 0:
             run_serving(args)
+        return
+    if args.workload == "large":
+        if rank == 0:
+            run_large(args)
         return
     if world > 1:
         import datetime

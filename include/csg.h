@@ -41,7 +41,7 @@ enum {
 };
 
 typedef struct csg_dims {
-    int32_t L;        /* lattice side: even, 4..24 */
+    int32_t L;        /* lattice side: even, 4..128 (L > 24: streaming engine) */
     int32_t n_words;  /* disorder samples / 32 */
     int32_t n_copies; /* independent copies per sample: 1 or 2 */
     int32_t n_temps;  /* temperatures: multiple of 4, 4..64 */
@@ -54,7 +54,10 @@ typedef struct csg_schedule {
 } csg_schedule;
 
 enum {
-    CSG_MEASURE_M = 1 /* also accumulate magnetisations at measurements */
+    CSG_MEASURE_M = 1,   /* also accumulate magnetisations at measurements */
+    CSG_ENGINE_STREAM = 2 /* run the streaming engine (state in global memory, one
+                             launch per colour) even where the cluster-resident
+                             kernel fits; it always runs for L > 24 */
 };
 
 typedef struct csg_config {
@@ -63,7 +66,7 @@ typedef struct csg_config {
     double H;                /* external field, 0 <= H <= 4 (eamsim.cu:520) */
     uint64_t seed;           /* Philox key of the whole simulation */
     const double* betas;     /* n_temps inverse temperatures (host); exchanges pair t, t+1 */
-    int32_t flags;           /* CSG_MEASURE_M */
+    int32_t flags;           /* CSG_MEASURE_M | CSG_ENGINE_STREAM */
     int32_t swap_log_rounds; /* keep accepted-exchange masks of this many rounds (tests) */
     int32_t word0;           /* global index of the first sample word (Philox counter word
                                 2): a simulation split into shards of words with matching

@@ -22,6 +22,7 @@ PKG_DIR = pathlib.Path(__file__).resolve().parent
 LIB_PATH = PKG_DIR / "libcsg.so"
 
 CSG_MEASURE_M = 1
+CSG_ENGINE_STREAM = 2
 _lib = None
 
 

@@ -13,6 +13,7 @@
 #include "philox.cuh"
 #include "pt_kernel.cuh"
 #include "aux_kernels.cuh"
+#include "stream_kernels.cuh"
 
 namespace {
 
@@ -39,14 +40,23 @@ namespace {
             return fail(CSG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
-bool lattice_supported(int L) { return L >= 4 && L <= 24 && L % 2 == 0; }
+constexpr int kMaxResidentL = 24;  // largest L of the cluster-resident kernel
+constexpr int kMaxL = 128;         // largest L of the streaming engine
+
+bool lattice_supported(int L) { return L >= 4 && L <= kMaxL && L % 2 == 0; }
+
+// Lattices whose quads do not fit in a cluster's shared memory run on the
+// streaming engine; CSG_ENGINE_STREAM selects it for any L.
+bool use_stream(const csg_config& c) {
+    return c.dims.L > kMaxResidentL || (c.flags & CSG_ENGINE_STREAM);
+}
 
 int validate(const csg_config* cfg) {
     if (!cfg) return fail(CSG_ERR_ARG, "null configuration");
     const csg_dims& d = cfg->dims;
     if (d.L < 4 || d.L % 2 != 0) return fail(CSG_ERR_ARG, "L must be even and >= 4");
     if (!lattice_supported(d.L))
-        return fail(CSG_ERR_UNSUPPORTED, "L=" + std::to_string(d.L) + " outside 4..24");
+        return fail(CSG_ERR_UNSUPPORTED, "L=" + std::to_string(d.L) + " outside 4..128");
     if (d.n_words < 1) return fail(CSG_ERR_ARG, "n_words must be >= 1");
     if (d.n_copies != 1 && d.n_copies != 2) return fail(CSG_ERR_ARG, "n_copies must be 1 or 2");
     if (d.n_temps < 4 || d.n_temps > csg::kMaxT || d.n_temps % 4 != 0)
@@ -183,6 +193,11 @@ void fill_launch(cudaLaunchConfig_t& lc, cudaLaunchAttribute* attr, int W, const
 int make_plan(const csg_config& cfg, bool gen, Plan& out, int forced_qc = 0) {
     const int L = cfg.dims.L, W = cfg.dims.n_words;
     const int G = cfg.dims.n_copies * cfg.dims.n_temps / 4;
+    if (use_stream(cfg)) {  // fixed launch shapes, nothing to plan
+        out = Plan{};
+        out.TPQ = csg::kStreamThreads;
+        return CSG_OK;
+    }
     const int tpq = csg::tpq_for(L);
     const bool has_m = gen || (cfg.flags & CSG_MEASURE_M);
     KernelFn fn = select_kernel(L, gen);
@@ -263,9 +278,150 @@ int fill_params(const csg_config& cfg, csg::PtParams& P, bool& gen) {
 
 constexpr int64_t kSweepsPerLaunch = 1024;
 
+// ---------------------------------------------------------------------------
+// Streaming engine (stream_kernels.cuh): scratch layout and the launch
+// sequence of one sweep.
+// ---------------------------------------------------------------------------
+struct StreamLayout {
+    int nblk = 0, nblk2 = 0;
+    size_t e_part = 0, m_part = 0, d_part = 0, energy = 0, magn = 0, masks = 0, bytes = 0;
+};
+
+StreamLayout stream_layout(const csg_config& c) {
+    const csg_dims& d = c.dims;
+    const size_t N = (size_t)d.L * d.L * d.L, Q = (size_t)d.n_temps / 4;
+    const size_t spb = csg::kStreamSitesPerBlock;
+    StreamLayout s;
+    s.nblk = (int)((N / 2 + spb - 1) / spb);
+    s.nblk2 = (int)((N + spb - 1) / spb);
+    const size_t quads = (size_t)d.n_words * d.n_copies * Q;
+    const size_t planes = (size_t)d.n_words * d.n_copies * d.n_temps;
+    auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    size_t off = 0;
+    s.e_part = off, off += up(quads * s.nblk * 128 * 4);
+    s.m_part = off, off += up(quads * 2 * s.nblk * 128 * 4);
+    s.d_part = off, off += up((size_t)d.n_words * Q * s.nblk2 * 128 * 4);
+    s.energy = off, off += up(planes * 32 * 4);
+    s.magn = off, off += up(planes * 32 * 4);
+    s.masks = off, off += up(planes * 4);
+    s.bytes = off;
+    return s;
+}
+
+using ColourLaunch = void (*)(const csg::StreamParams&, dim3, int, long long, cudaStream_t);
+
+template <bool G, bool E, bool M>
+void launch_colour(const csg::StreamParams& S, dim3 grid, int p, long long s, cudaStream_t st) {
+    csg::stream_colour_kernel<G, E, M><<<grid, csg::kStreamThreads, 0, st>>>(S, p, s);
+}
+
+ColourLaunch colour_launch(bool gen, bool acc_e, bool acc_m) {
+    static const ColourLaunch fns[8] = {
+        launch_colour<false, false, false>, launch_colour<false, false, true>,
+        launch_colour<false, true, false>,  launch_colour<false, true, true>,
+        launch_colour<true, false, false>,  launch_colour<true, false, true>,
+        launch_colour<true, true, false>,   launch_colour<true, true, true>};
+    return fns[(gen ? 4 : 0) + (acc_e ? 2 : 0) + (acc_m ? 1 : 0)];
+}
+
+// Same schedule, Philox counters and arithmetic as the resident kernel's sweep
+// loop; per sweep: colour 0, colour 1 (energies, magnetisations when needed),
+// then the exchange decisions, the masked exchange and the measurement.
+int run_stream(const csg_config& cfg, uint32_t* spins, const uint32_t* bonds,
+               const csg_device_obs* obs, int64_t sweep0, int64_t n_sweeps, cudaStream_t st) {
+    csg::PtParams tp;
+    bool gen = false;
+    fill_params(cfg, tp, gen);
+    const csg_dims& d = cfg.dims;
+    const StreamLayout lay = stream_layout(cfg);
+    csg::StreamParams S;
+    std::memset(&S, 0, sizeof(S));
+    S.spins = spins;
+    S.bonds = bonds;
+    S.L = d.L;
+    S.W = d.n_words;
+    S.C = d.n_copies;
+    S.T = d.n_temps;
+    S.Q = d.n_temps / 4;
+    S.nblk = lay.nblk;
+    S.nblk2 = lay.nblk2;
+    S.k0 = tp.k0;
+    S.k1 = tp.k1;
+    S.word0 = tp.word0;
+    S.H = tp.H;
+    S.tab = tp.tab;
+    csg::StreamObs O{};
+    unsigned long long *boundary = nullptr, *swap_acc = nullptr;
+    unsigned int* swap_log = nullptr;
+    long long log_rounds = 0, round0 = 0;
+    if (obs) {
+        O.e_sum = reinterpret_cast<long long*>(obs->e_sum);
+        O.m_sum = reinterpret_cast<long long*>(obs->m_sum);
+        O.q_sum = reinterpret_cast<long long*>(obs->q_sum);
+        O.q2_sum = reinterpret_cast<long long*>(obs->q2_sum);
+        O.q4_sum = reinterpret_cast<unsigned long long*>(obs->q4_sum);
+        O.hist = obs->hist;
+        O.e_last = obs->e_last;
+        O.m_last = obs->m_last;
+        O.d_last = obs->d_last;
+        boundary = reinterpret_cast<unsigned long long*>(obs->boundary);
+        swap_acc = reinterpret_cast<unsigned long long*>(obs->swap_acc);
+        swap_log = obs->swap_log;
+        log_rounds = obs->swap_log_rounds;
+        round0 = obs->swap_round0;
+    }
+    char* base = nullptr;
+    CSG_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&base), lay.bytes, st));
+    S.e_part = reinterpret_cast<int*>(base + lay.e_part);
+    S.m_part = reinterpret_cast<int*>(base + lay.m_part);
+    S.d_part = reinterpret_cast<int*>(base + lay.d_part);
+    S.energy = reinterpret_cast<int*>(base + lay.energy);
+    S.magn = reinterpret_cast<int*>(base + lay.magn);
+    S.masks = reinterpret_cast<uint32_t*>(base + lay.masks);
+
+    const long N = (long)d.L * d.L * d.L;
+    const unsigned W = (unsigned)d.n_words, C = (unsigned)d.n_copies, Q = (unsigned)S.Q;
+    const dim3 g_colour(W * C * Q, (unsigned)lay.nblk);
+    const dim3 g_exchange(W * C, (unsigned)((N + 255) / 256));
+    const dim3 g_overlap(W * Q, (unsigned)lay.nblk2);
+    const int64_t sps = cfg.sched.sweeps_per_swap, spm = cfg.sched.sweeps_per_meas;
+    cudaError_t ce = cudaSuccess;
+    for (int64_t i = 0; i < n_sweeps && ce == cudaSuccess; ++i) {
+        const long long s = sweep0 + i;
+        const bool do_swap = sps > 0 && (s + 1) % sps == 0;
+        const bool do_meas = spm > 0 && (s + 1) % spm == 0 && s >= cfg.sched.meas_start;
+        const bool need_E = do_swap || do_meas;
+        const bool need_M = need_E && (gen || (do_meas && (cfg.flags & CSG_MEASURE_M)));
+        colour_launch(gen, false, need_M)(S, g_colour, 0, s, st);
+        colour_launch(gen, need_E, need_M)(S, g_colour, 1, s, st);
+        if (need_E) {
+            const long long round = do_swap ? (s + 1) / sps - 1 : 0;
+            const int par = (int)(round & 1);
+            csg::stream_decide_kernel<<<W * C, 256, 0, st>>>(S, s, par, need_M, do_swap, boundary,
+                                                              swap_acc, swap_log, round - round0,
+                                                              log_rounds);
+            if (do_swap) csg::stream_exchange_kernel<<<g_exchange, 256, 0, st>>>(S, par);
+            if (do_meas && obs) {
+                if (C == 2) csg::stream_overlap_kernel<<<g_overlap, csg::kStreamThreads, 0, st>>>(S);
+                csg::stream_measure_kernel<<<W, 256, 0, st>>>(S, need_M, O);
+            }
+        }
+        ce = cudaGetLastError();
+    }
+    const cudaError_t ce2 = cudaFreeAsync(base, st);
+    if (ce != cudaSuccess) return fail(CSG_ERR_CUDA, std::string("stream launch: ") + cudaGetErrorString(ce));
+    if (ce2 != cudaSuccess) return fail(CSG_ERR_CUDA, std::string("cudaFreeAsync: ") + cudaGetErrorString(ce2));
+    return CSG_OK;
+}
+
 int run_device(const csg_config& cfg, uint32_t* spins, const uint32_t* bonds,
                const csg_device_obs* obs, int64_t sweep0, int64_t n_sweeps, cudaStream_t st,
                int forced_qc = 0, long long* sweep_dev = nullptr, const Plan* plan_in = nullptr) {
+    if (use_stream(cfg)) {
+        if (sweep_dev)
+            return fail(CSG_ERR_UNSUPPORTED, "the streaming engine takes no device sweep counter");
+        return run_stream(cfg, spins, bonds, obs, sweep0, n_sweeps, st);
+    }
     csg::PtParams P;
     bool gen = false;
     fill_params(cfg, P, gen);
@@ -655,9 +811,11 @@ int csg_obs_records(csg_engine* e, float* rec, size_t n_floats) {
     if (!rc) rc = dalloc(&dp, nP);
     std::vector<int> he(nE), hm(nE), hd(nD), hp(nP);
     if (!rc) {
-        const int warps = 4;
+        // 3L counters per lane; as many warps as fit in 48 KB (4 up to L = 32)
+        const size_t per_warp = (size_t)32 * 3 * L * sizeof(int);
+        const int warps = (int)std::max<size_t>(1, std::min<size_t>(4, 49152 / per_warp));
         const unsigned blocks = (unsigned)((W * T + warps - 1) / warps);
-        const size_t sh = (size_t)warps * 32 * 3 * L * sizeof(int);
+        const size_t sh = (size_t)warps * per_warp;
         csg::measure_kernel<<<blocks, warps * 32, sh, e->stream>>>(e->spins, e->bonds, L, W, T, de,
                                                                    dm, dd, dp);
         cudaError_t ce = cudaGetLastError();
@@ -893,6 +1051,11 @@ int csg_batch_create(const csg_config* cfgs, int32_t n, csg_batch** out) {
     for (int i = 0; i < n && rc == CSG_OK; ++i) {
         csg_engine* e = nullptr;
         rc = csg_engine_create(&cfgs[i], &e);
+        if (rc == CSG_OK && use_stream(cfgs[i])) {
+            csg_engine_destroy(e);
+            rc = fail(CSG_ERR_UNSUPPORTED,
+                      "batch members need the cluster-resident kernel (L <= 24, no CSG_ENGINE_STREAM)");
+        }
         if (rc == CSG_OK) b->eng.push_back(e);
     }
     if (rc == CSG_OK && cudaStreamCreateWithFlags(&b->main, cudaStreamNonBlocking) != cudaSuccess)
@@ -1073,7 +1236,8 @@ size_t footprint_bytes(const csg_config& c) {
     const size_t nh = d.n_copies == 2 ? (size_t)d.n_temps * (N + 1) : 0;
     return (size_t)d.n_words * d.n_copies * d.n_temps * N * 4 + (size_t)d.n_words * 3 * N * 4 +
            ne * (8 + 8 + 4 + 4) + nq * (8 + 8 + 16 + 4) + nh * 4 +
-           (size_t)d.n_copies * d.n_temps * 8 + (size_t)c.swap_log_rounds * ne / 32 * 4 + 8;
+           (size_t)d.n_copies * d.n_temps * 8 + (size_t)c.swap_log_rounds * ne / 32 * 4 + 8 +
+           (use_stream(c) ? stream_layout(c).bytes : 0);
 }
 
 }  // namespace

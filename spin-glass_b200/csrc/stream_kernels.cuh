@@ -1,0 +1,377 @@
+// stream_kernels.cuh — parallel tempering for lattices whose temperature quads
+// do not fit in shared memory (L > 24), streamed through L2/HBM.
+//
+// One sweep = two colour launches (stream_colour_kernel), then, when the
+// schedule asks for it, the exchange decisions (stream_decide_kernel), the
+// masked exchange (stream_exchange_kernel) and the overlap measurement
+// (stream_overlap_kernel + stream_measure_kernel).  The arithmetic of a site
+// update, of the energies and of the exchange rule is the same as the
+// cluster-resident kernel's (pt_kernel.cuh), so results are bit-identical to
+// it and to the CPU oracle.  Per-block partial sums (no atomics on the sweep
+// path) are reduced by the decision and measurement kernels.
+#pragma once
+#include <cstdint>
+
+#include "philox.cuh"
+#include "pt_kernel.cuh"
+
+namespace csg {
+
+constexpr int kStreamThreads = 256;
+constexpr int kStreamSPT = 8;  // sites of one colour per thread per launch
+constexpr int kStreamSitesPerBlock = kStreamThreads * kStreamSPT;
+constexpr int kStreamNLV = bit_length(6 * kStreamSPT);  // bits of a per-thread bond count
+constexpr int kStreamNLM = bit_length(kStreamSPT);      // bits of a per-thread site count
+
+struct StreamParams {
+    uint32_t* spins;
+    const uint32_t* bonds;
+    int* e_part;  // [W*C*Q][nblk][4][32] unsatisfied-bond partial sums
+    int* m_part;  // [W*C*Q][2 colours][nblk][4][32] spin-up partial sums
+    int* d_part;  // [W*Q][nblk2][4][32] differing-site partial sums
+    int* energy;  // [W][C][T][32] bond energies after the exchange
+    int* magn;    // [W][C][T][32]
+    uint32_t* masks;  // [W][C][T] accepted-sample masks of the current round
+    int L, W, C, T, Q;
+    int nblk;   // blocks per quad and colour
+    int nblk2;  // blocks per quad for the overlap (over all N sites)
+    uint32_t k0, k1, word0;
+    double H;
+    PtTables tab;
+};
+
+// Measurement accumulators (layouts as in PtParams / csg_device_obs).
+struct StreamObs {
+    long long* e_sum;
+    long long* m_sum;
+    long long* q_sum;
+    long long* q2_sum;
+    unsigned long long* q4_sum;
+    unsigned int* hist;
+    int* e_last;
+    int* m_last;
+    int* d_last;
+};
+
+__device__ __forceinline__ void site_coords(int n, int L, int& x, int& y, int& z, int p) {
+    const int LH = L / 2;
+    z = n / (L * LH);
+    const int rem = n - z * (L * LH);
+    y = rem / LH;
+    const int h = rem - y * LH;
+    x = 2 * h + ((y + z + p) & 1);
+}
+
+// One colour of one sweep.  blockIdx.x = quad (w, c, q), blockIdx.y = block
+// of kStreamSitesPerBlock sites of that colour; each thread updates
+// kStreamSPT sites in the 4 planes of the quad.  Consecutive blocks take the
+// quads of one word at the same sites, so the word's bonds are read once from
+// DRAM and then from L2.
+template <bool GEN_H, bool ACC_E, bool ACC_M>
+__global__ void __launch_bounds__(kStreamThreads) stream_colour_kernel(const __grid_constant__ StreamParams P,
+                                                                       int p, long long s) {
+    const int L = P.L, LH = L / 2;
+    const long N = (long)L * L * L, NH = N / 2;
+    const int gq = blockIdx.x;
+    const int w = gq / (P.C * P.Q), c = (gq / P.Q) % P.C, q = gq % P.Q;
+    uint4* Sq = reinterpret_cast<uint4*>(P.spins) + (size_t)gq * N;
+    uint4* Sc = Sq + p * NH;
+    const uint4* So = Sq + (1 - p) * NH;
+    const uint32_t* Fw = P.bonds + (size_t)w * 3 * N;
+    const uint32_t* Fc = Fw + p * NH;
+    const uint32_t* Fo = Fw + (1 - p) * NH;
+    const uint32_t ctr3 = kTagSweep | ((uint32_t)c << 8) | (uint32_t)q;
+    const uint32_t wg = (uint32_t)w + P.word0;
+    const int lane = threadIdx.x & 31;
+    uint32_t th0[4], th1[4], th2[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int t = 4 * q + k;
+        th0[k] = P.tab.thr[t][0][0];
+        th1[k] = P.tab.thr[t][0][1];
+        th2[k] = P.tab.thr[t][0][2];
+    }
+    constexpr int NLV = kStreamNLV;
+    constexpr int NLM = kStreamNLM;
+    uint32_t ecnt[4][NLV], mcnt[4][NLM];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+#pragma unroll
+        for (int l = 0; l < NLV; ++l) ecnt[k][l] = 0;
+#pragma unroll
+        for (int l = 0; l < NLM; ++l) mcnt[k][l] = 0;
+    }
+    const long n_base = (long)blockIdx.y * kStreamSitesPerBlock + threadIdx.x;
+#pragma unroll 1
+    for (int m = 0; m < kStreamSPT; ++m) {
+        const long n = n_base + (long)m * kStreamThreads;
+        uint32_t wd[4][4] = {};
+        uint32_t up[4] = {0, 0, 0, 0};
+        if (n < NH) {
+            int x, y, z;
+            site_coords((int)n, L, x, y, z, p);
+            const int h = x >> 1, o = x & 1;
+            const int hxm = o ? h : (h == 0 ? LH - 1 : h - 1);
+            const int hxp = o ? (h == LH - 1 ? 0 : h + 1) : h;
+            const int ym = y == 0 ? L - 1 : y - 1, yp = y == L - 1 ? 0 : y + 1;
+            const int zm = z == 0 ? L - 1 : z - 1, zp = z == L - 1 ? 0 : z + 1;
+            const long row = ((long)z * L + y) * LH;
+            const long nxm = row + hxm, nxp = row + hxp;
+            const long nym = ((long)z * L + ym) * LH + h, nyp = ((long)z * L + yp) * LH + h;
+            const long nzm = ((long)zm * L + y) * LH + h, nzp = ((long)zp * L + y) * LH + h;
+            const uint4 cv = Sc[n];
+            const uint4 a0 = __ldg(So + nxm), a1 = __ldg(So + nxp), a2 = __ldg(So + nym),
+                        a3 = __ldg(So + nyp), a4 = __ldg(So + nzm), a5 = __ldg(So + nzp);
+            const uint32_t f0 = __ldg(Fo + nxm), f1 = __ldg(Fc + n);
+            const uint32_t f2 = __ldg(Fo + N + nym), f3 = __ldg(Fc + N + n);
+            const uint32_t f4 = __ldg(Fo + 2 * N + nzm), f5 = __ldg(Fc + 2 * N + n);
+            const u32x4 r = philox4x32_10((uint32_t)(((long)z * L + y) * L + x), (uint32_t)s, wg,
+                                          ctr3, P.k0, P.k1);
+            const uint32_t rr[4] = {r.v0, r.v1, r.v2, r.v3};
+            uint32_t cw[4] = {cv.x, cv.y, cv.z, cv.w};
+            const uint32_t n0w[4] = {a0.x, a0.y, a0.z, a0.w}, n1w[4] = {a1.x, a1.y, a1.z, a1.w};
+            const uint32_t n2w[4] = {a2.x, a2.y, a2.z, a2.w}, n3w[4] = {a3.x, a3.y, a3.z, a3.w};
+            const uint32_t n4w[4] = {a4.x, a4.y, a4.z, a4.w}, n5w[4] = {a5.x, a5.y, a5.z, a5.w};
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const uint32_t s0 = cw[k];
+                const uint32_t u0 = s0 ^ n0w[k] ^ f0, u1 = s0 ^ n1w[k] ^ f1;
+                const uint32_t u2 = s0 ^ n2w[k] ^ f2, u3 = s0 ^ n3w[k] ^ f3;
+                const uint32_t u4 = s0 ^ n4w[k] ^ f4, u5 = s0 ^ n5w[k] ^ f5;
+                const uint32_t sa = u0 ^ u1 ^ u2, ca = maj3(u0, u1, u2);
+                const uint32_t sb = u3 ^ u4 ^ u5, cb = maj3(u3, u4, u5);
+                uint32_t fl;
+                if constexpr (GEN_H)
+                    fl = flip_gen(s0, sa, ca, sb, cb, rr[k], &P.tab.thr[4 * q + k][0][0],
+                                  &P.tab.ucut[4 * q + k][0]);
+                else
+                    fl = flip_h0(sa, ca, sb, cb, rr[k], th0[k], th1[k], th2[k]);
+                cw[k] = s0 ^ fl;
+                wd[k][0] = sa ^ fl;
+                wd[k][1] = sb ^ fl;
+                wd[k][2] = ca ^ fl;
+                wd[k][3] = cb ^ fl;
+                up[k] = cw[k];
+            }
+            Sc[n] = make_uint4(cw[0], cw[1], cw[2], cw[3]);
+        }
+        if constexpr (ACC_E) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) vc_add_site<NLV>(ecnt[k], wd[k][0], wd[k][1], wd[k][2], wd[k][3]);
+        }
+        if constexpr (ACC_M) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                uint32_t carry = up[k];
+#pragma unroll
+                for (int l = 0; l < NLM; ++l) {
+                    const uint32_t t = mcnt[k][l] & carry;
+                    mcnt[k][l] ^= carry;
+                    carry = t;
+                }
+            }
+        }
+    }
+    __shared__ int sred[2][4][32];
+    if (ACC_E || ACC_M) {
+        for (int i = threadIdx.x; i < 2 * 4 * 32; i += kStreamThreads) (&sred[0][0][0])[i] = 0;
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if constexpr (ACC_E) atomicAdd(&sred[0][k][lane], column_count<NLV>(ecnt[k], lane));
+            if constexpr (ACC_M) atomicAdd(&sred[1][k][lane], column_count<NLM>(mcnt[k], lane));
+        }
+        __syncthreads();
+        if (threadIdx.x < 128) {
+            const int k = threadIdx.x >> 5;
+            if constexpr (ACC_E)
+                P.e_part[(((size_t)gq * P.nblk + blockIdx.y) * 4 + k) * 32 + lane] = sred[0][k][lane];
+            if constexpr (ACC_M)
+                P.m_part[((((size_t)gq * 2 + p) * P.nblk + blockIdx.y) * 4 + k) * 32 + lane] =
+                    sred[1][k][lane];
+        }
+    }
+}
+
+// Exchange decisions of one round: block = (w, c), one warp per pair.  Also
+// totals the energies (and magnetisations) of every plane and swaps them for
+// the accepted samples.
+__global__ void stream_decide_kernel(const __grid_constant__ StreamParams P, long long s, int par,
+                                     bool need_M, bool do_swap, unsigned long long* boundary,
+                                     unsigned long long* swap_acc, unsigned int* swap_log,
+                                     long long log_row, long long log_rows) {
+    const int wc = blockIdx.x, w = wc / P.C, c = wc % P.C;
+    const int T = P.T, N = P.L * P.L * P.L;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    int* E = P.energy + (size_t)wc * T * 32;
+    int* M = P.magn + (size_t)wc * T * 32;
+    for (int t = warp; t < T; t += nwarps) {
+        const int q = t >> 2, k = t & 3, gq = wc * P.Q + q;
+        int u = 0, up = 0;
+        for (int b = 0; b < P.nblk; ++b) {
+            u += P.e_part[(((size_t)gq * P.nblk + b) * 4 + k) * 32 + lane];
+            if (need_M)
+                for (int pp = 0; pp < 2; ++pp)
+                    up += P.m_part[((((size_t)gq * 2 + pp) * P.nblk + b) * 4 + k) * 32 + lane];
+        }
+        E[t * 32 + lane] = 2 * u - 3 * N;
+        M[t * 32 + lane] = need_M ? 2 * up - N : 0;
+    }
+    __syncthreads();
+    if (!do_swap) return;
+    const uint32_t wg = (uint32_t)w + P.word0;
+    for (int t = par + 2 * warp; t + 1 < T; t += 2 * nwarps) {
+        const int e0 = E[t * 32 + lane], e1 = E[(t + 1) * 32 + lane];
+        const int m0 = M[t * 32 + lane], m1 = M[(t + 1) * 32 + lane];
+        const u32x4 r = philox4x32_10((uint32_t)(lane >> 1), (uint32_t)s, wg,
+                                      kTagSwap | ((uint32_t)c << 8) | (uint32_t)t, P.k0, P.k1);
+        const uint32_t lo = (lane & 1) ? r.v2 : r.v0;
+        const uint32_t hi = (lane & 1) ? r.v3 : r.v1;
+        const double uu = (double)((((unsigned long long)hi << 32) | lo) >> 11) * 0x1p-53;
+        const double dE = __dsub_rn((double)(e0 - e1), __dmul_rn(P.H, (double)(m0 - m1)));
+        const double delta = __dmul_rn(__dsub_rn(P.tab.beta[t], P.tab.beta[t + 1]), dE);
+        bool acc = true;
+        if (delta < 0.0) {
+            const double pr = exp(delta);
+            if (boundary && fabs(uu - pr) <= pr * 0x1p-40) atomicAdd(boundary, 1ull);
+            acc = uu < pr;
+        }
+        const uint32_t mask = __ballot_sync(0xFFFFFFFFu, acc);
+        if (acc) {
+            E[t * 32 + lane] = e1;
+            E[(t + 1) * 32 + lane] = e0;
+            M[t * 32 + lane] = m1;
+            M[(t + 1) * 32 + lane] = m0;
+        }
+        if (lane == 0) {
+            P.masks[(size_t)wc * T + t] = mask;
+            if (swap_acc) atomicAdd(&swap_acc[(size_t)c * T + t], (unsigned long long)__popc(mask));
+            if (swap_log && log_row >= 0 && log_row < log_rows)
+                swap_log[(((size_t)log_row * P.W + w) * P.C + c) * T + t] = mask;
+        }
+    }
+    // pairs that do not take part in this round keep a zero mask
+    for (int t = threadIdx.x; t < T; t += blockDim.x)
+        if (((t - par) & 1) || t + 1 >= T) P.masks[(size_t)wc * T + t] = 0;
+}
+
+// Masked exchange: a thread takes one site of one (w, c) and every quad of it,
+// so both words of every pair (also across quads) are its own.
+__global__ void stream_exchange_kernel(const __grid_constant__ StreamParams P, int par) {
+    const long N = (long)P.L * P.L * P.L;
+    const int wc = blockIdx.x;
+    const long n = (long)blockIdx.y * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    uint4* base = reinterpret_cast<uint4*>(P.spins) + (size_t)wc * P.Q * N + n;
+    const uint32_t* mk = P.masks + (size_t)wc * P.T;
+    if (par == 0) {  // pairs (0,1), (2,3) inside every quad
+        for (int q = 0; q < P.Q; ++q) {
+            uint4 v = base[(size_t)q * N];
+            const uint32_t d0 = (v.x ^ v.y) & mk[4 * q], d1 = (v.z ^ v.w) & mk[4 * q + 2];
+            v.x ^= d0; v.y ^= d0; v.z ^= d1; v.w ^= d1;
+            base[(size_t)q * N] = v;
+        }
+        return;
+    }
+    // odd rounds: (1,2) inside a quad, (3 of quad q, 0 of quad q+1) across quads
+    uint4 cur = base[0];
+    for (int q = 0; q < P.Q; ++q) {
+        const uint32_t d = (cur.y ^ cur.z) & mk[4 * q + 1];
+        cur.y ^= d;
+        cur.z ^= d;
+        if (q + 1 < P.Q) {
+            uint4 nxt = base[(size_t)(q + 1) * N];
+            const uint32_t e = (cur.w ^ nxt.x) & mk[4 * q + 3];
+            cur.w ^= e;
+            nxt.x ^= e;
+            base[(size_t)q * N] = cur;
+            cur = nxt;
+        } else {
+            base[(size_t)q * N] = cur;
+        }
+    }
+}
+
+// Overlap partial sums: blockIdx.x = (w, q), blockIdx.y = block of sites;
+// each thread kStreamSPT sites.
+__global__ void __launch_bounds__(kStreamThreads) stream_overlap_kernel(const __grid_constant__ StreamParams P) {
+    const long N = (long)P.L * P.L * P.L;
+    const int wq = blockIdx.x, w = wq / P.Q, q = wq % P.Q;
+    const int lane = threadIdx.x & 31;
+    const uint4* A = reinterpret_cast<const uint4*>(P.spins) + ((size_t)(w * P.C + 0) * P.Q + q) * N;
+    const uint4* B = reinterpret_cast<const uint4*>(P.spins) + ((size_t)(w * P.C + 1) * P.Q + q) * N;
+    constexpr int NL = kStreamNLM;
+    uint32_t dc[4][NL];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int l = 0; l < NL; ++l) dc[k][l] = 0;
+    const long n_base = (long)blockIdx.y * kStreamSitesPerBlock + threadIdx.x;
+    for (int m = 0; m < kStreamSPT; ++m) {
+        const long n = n_base + (long)m * kStreamThreads;
+        uint4 x = make_uint4(0, 0, 0, 0);
+        if (n < N) {
+            const uint4 a = __ldg(A + n), b = __ldg(B + n);
+            x = make_uint4(a.x ^ b.x, a.y ^ b.y, a.z ^ b.z, a.w ^ b.w);
+        }
+        const uint32_t xs[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            uint32_t carry = xs[k];
+#pragma unroll
+            for (int l = 0; l < NL; ++l) {
+                const uint32_t t = dc[k][l] & carry;
+                dc[k][l] ^= carry;
+                carry = t;
+            }
+        }
+    }
+    __shared__ int sred[4][32];
+    for (int i = threadIdx.x; i < 128; i += kStreamThreads) (&sred[0][0])[i] = 0;
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 4; ++k) atomicAdd(&sred[k][lane], column_count<NL>(dc[k], lane));
+    __syncthreads();
+    if (threadIdx.x < 128) {
+        const int k = threadIdx.x >> 5;
+        P.d_part[(((size_t)wq * P.nblk2 + blockIdx.y) * 4 + k) * 32 + lane] = sred[k][lane];
+    }
+}
+
+// Measurement accumulators from the energies and the overlap partials:
+// block = w, thread = (t, sample).
+__global__ void stream_measure_kernel(const __grid_constant__ StreamParams P, bool need_M,
+                                      StreamObs O) {
+    const int w = blockIdx.x, T = P.T, N = P.L * P.L * P.L;
+    for (int i = threadIdx.x; i < P.C * T * 32; i += blockDim.x) {
+        const size_t o = (size_t)w * P.C * T * 32 + i;
+        const int e = P.energy[o], m = P.magn[o];
+        if (O.e_sum) atomicAdd(reinterpret_cast<unsigned long long*>(O.e_sum + o), (unsigned long long)(long long)e);
+        if (O.e_last) O.e_last[o] = e;
+        if (need_M) {
+            if (O.m_sum) atomicAdd(reinterpret_cast<unsigned long long*>(O.m_sum + o), (unsigned long long)(long long)m);
+            if (O.m_last) O.m_last[o] = m;
+        }
+    }
+    if (P.C != 2) return;
+    for (int i = threadIdx.x; i < T * 32; i += blockDim.x) {
+        const int t = i >> 5, b = i & 31, q = t >> 2, k = t & 3;
+        int D = 0;
+        for (int blk = 0; blk < P.nblk2; ++blk)
+            D += P.d_part[((((size_t)(w * P.Q + q)) * P.nblk2 + blk) * 4 + k) * 32 + b];
+        const long long Qv = (long long)N - 2LL * D;
+        const unsigned long long q2 = (unsigned long long)(Qv * Qv);
+        const size_t o = ((size_t)w * T + t) * 32 + b;
+        if (O.q_sum) atomicAdd(reinterpret_cast<unsigned long long*>(O.q_sum + o), (unsigned long long)Qv);
+        if (O.q2_sum) atomicAdd(reinterpret_cast<unsigned long long*>(O.q2_sum + o), q2);
+        if (O.q4_sum) {
+            const unsigned long long lo = q2 * q2, hi = __umul64hi(q2, q2);
+            atomicAdd(O.q4_sum + 2 * o, lo & 0xFFFFFFFFull);
+            atomicAdd(O.q4_sum + 2 * o + 1, (lo >> 32) | (hi << 32));
+        }
+        if (O.hist) atomicAdd(&O.hist[(size_t)t * (N + 1) + D], 1u);
+        if (O.d_last) O.d_last[o] = D;
+    }
+}
+
+}  // namespace csg

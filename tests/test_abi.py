@@ -51,7 +51,7 @@ def test_struct_layouts_match_header(tmp_path, csg):
 
 @pytest.mark.parametrize("kw,msg", [
     (dict(L=7), "even"),
-    (dict(L=32), "outside"),
+    (dict(L=130), "outside"),
     (dict(n_words=0), "n_words"),
     (dict(n_copies=3), "n_copies"),
     (dict(T=6), "multiple of 4"),
