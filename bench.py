@@ -20,9 +20,11 @@ import importlib.util
 import json
 import os
 import pathlib
+import re
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -168,6 +170,47 @@ def cpu_sample(target_s: float, n_threads: int = 0) -> dict:
                       f"{el:.1f} s, {cores} OpenMP threads"}
 
 
+def _t_e(text: str):
+    m = re.findall(r"t_e = *([0-9.]+) ps", text)
+    return float(m[-1]) if m else None
+
+
+def reference_cuda_baseline(timeout_s: float = 300.0) -> dict:
+    """The reference program itself, built for sm_100a by oracle/build_ref.sh
+    (only its L and SPFILE constants set: L=16, SPFILE=16384), run once on this
+    GPU with its shipped configuration (2048 samples, 2 copies, 24 temperatures
+    of its ladder, exchange every 16 sweeps, measurement every 1024); its own
+    t_e printout (ps per attempt) gives attempts/ns.  Beside it, our csg
+    command on the same configuration and sweep count."""
+    exe = ROOT / "oracle" / "_ref" / "csg_ref_L16"
+    ours = ROOT / "spin-glass_b200" / "csg"
+    out = {"config": "L=16, 2048 samples, 2 copies, 24 temperatures (reference ladder), "
+                     "exchange every 16 sweeps, measurement every 1024, 16384 sweeps, "
+                     "through each program's command line",
+           "unit": METRIC}
+    if not exe.exists():
+        out["unavailable"] = "oracle/_ref/csg_ref_L16 not built (needs the reference sources)"
+        return out
+    with tempfile.TemporaryDirectory() as d:
+        for name, cmd_exe, conf in (("reference", exe, None), ("ours", ours, "SPFILE = 16384\n")):
+            sim = pathlib.Path(d) / name
+            sim.mkdir()
+            if conf:
+                (sim / "csg.conf").write_text(conf)
+            t0 = time.perf_counter()
+            try:
+                p = subprocess.run([str(cmd_exe), str(sim), "0"], cwd=d, capture_output=True,
+                                   text=True, timeout=timeout_s)
+                text, rc = p.stdout + p.stderr, p.returncode
+            except (OSError, subprocess.TimeoutExpired) as exc:
+                text, rc = str(exc), -1
+            wall = time.perf_counter() - t0
+            te = _t_e(text)
+            out[name] = {"value": 1000.0 / te if te and rc == 0 else None, "t_e_ps": te,
+                         "exit_code": rc, "wall_s": round(wall, 2)}
+    return out
+
+
 def run_reference(args, rank: int, world: int) -> None:
     if rank != 0:
         return
@@ -287,6 +330,7 @@ def run_ours(args, rank: int, world: int, dist) -> None:
             "clocks": clk.summary()}
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_sample(args.cpu_seconds)
+        line["reference_cuda"] = reference_cuda_baseline()
     print(json.dumps(line), flush=True)
 
 
