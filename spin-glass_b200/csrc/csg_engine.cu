@@ -832,6 +832,11 @@ int csg_obs_records(csg_engine* e, float* rec, size_t n_floats) {
     const int64_t N = (int64_t)L * L * L;
     const float H = (float)e->cfg.H;
     const double k = 2.0 * M_PI / L;
+    std::vector<double> cosv(L), sinv(L);  // the L phases exp(i k a), computed once
+    for (int a = 0; a < L; ++a) {
+        cosv[a] = std::cos(k * a);
+        sinv[a] = std::sin(k * a);
+    }
     for (int w = 0; w < W; ++w)
         for (int b = 0; b < 32; ++b)
             for (int t = 0; t < T; ++t) {
@@ -849,8 +854,8 @@ int csg_obs_records(csg_engine* e, float* rec, size_t n_floats) {
                     double re = 0.0, im = 0.0;
                     for (int a = 0; a < L; ++a) {
                         const int64_t P = (int64_t)L * L - 2 * (int64_t)hp[(i * 3 + dir) * L + a];
-                        re += (double)P * std::cos(k * a);
-                        im += (double)P * std::sin(k * a);
+                        re += (double)P * cosv[a];
+                        im += (double)P * sinv[a];
                     }
                     o[5 + dir] = (float)(re / (double)N);
                     o[8 + dir] = (float)(im / (double)N);

@@ -244,7 +244,9 @@ __device__ __forceinline__ uint32_t flip_gen(uint32_t s0, uint32_t sa, uint32_t 
 }
 
 // Shared-memory layout of one CTA (dynamic):
-//   uint4 quads[Qc][N]; int sE[Qc*4][32]; int sD[Qc*4][32];
+//   uint32 planes[Qc][4][N] (the 4 temperature planes of each quad as separate
+//   arrays, so that every access of one plane by a warp is conflict-free);
+//   int sE[Qc*4][32]; int sD[Qc*4][32];
 //   int sM[Qc*4][32]                      (only with magnetisations)
 //   uint32 sThr[Qc*4][2][7]; uint8 sUcut[Qc*4][2]   (only for H != 0)
 // The exchange masks of a round live in the first 2*Qc words of sD, which is
@@ -279,7 +281,17 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
     const int warp = tid >> 5, lane = tid & 31, nwarps = nthreads >> 5;
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    uint4* S = reinterpret_cast<uint4*>(smem_raw);
+    uint32_t* S = reinterpret_cast<uint32_t*>(smem_raw);  // planes[Qc][4][N]
+    // the 4 planes of a quad at one site
+    auto ld4 = [](const uint32_t* b, int i) {
+        return make_uint4(b[i], b[N + i], b[2 * N + i], b[3 * N + i]);
+    };
+    auto st4 = [](uint32_t* b, int i, uint4 v) {
+        b[i] = v.x;
+        b[N + i] = v.y;
+        b[2 * N + i] = v.z;
+        b[3 * N + i] = v.w;
+    };
     const bool has_M = GEN_H || (P.flags & kFlagMeasureM);
     int* sE = reinterpret_cast<int*>(smem_raw + (size_t)Qc * N * 16);
     int* sD = sE + Qc * 4 * 32;
@@ -292,7 +304,10 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
     const size_t qbase = ((size_t)w * C * Q + (size_t)rank * Qc) * N;
     {
         const uint4* src = reinterpret_cast<const uint4*>(P.spins) + qbase;
-        for (int i = tid; i < Qc * N; i += nthreads) S[i] = src[i];
+        for (int i = tid; i < Qc * N; i += nthreads) {
+            const int jj = i / N, n = i - jj * N;
+            st4(S + (size_t)jj * 4 * N, n, src[i]);
+        }
     }
     if constexpr (GEN_H) {
         for (int i = tid; i < Qc * 4 * 14; i += nthreads) {
@@ -318,7 +333,7 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
     }
     __syncthreads();
 
-    uint4* Sq = S + (size_t)j * N;
+    uint32_t* Sq = S + (size_t)j * 4 * N;
     const uint32_t* Fw = P.bonds + (size_t)w * 3 * N;
     const uint32_t ctr3 = kTagSweep | ((uint32_t)c << 8) | (uint32_t)q;
     const uint32_t wg = (uint32_t)w + P.word0;  // global sample word
@@ -347,8 +362,8 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
         // unsatisfied-bond counts into the energy counters
         auto colour_pass = [&](const int p, auto acc_tag) {
             constexpr bool ACC = decltype(acc_tag)::value;
-            uint4* Sc = Sq + p * NH;
-            const uint4* So = Sq + (1 - p) * NH;
+            uint32_t* Sc = Sq + p * NH;
+            const uint32_t* So = Sq + (1 - p) * NH;
             const uint32_t* Fc = Fw + p * NH;
             const uint32_t* Fo = Fw + (1 - p) * NH;
 #pragma unroll 1
@@ -375,9 +390,9 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
                         const int nym = (z * L + ym) * LH + h, nyp = (z * L + yp) * LH + h;
                         const int nzm = (zm * L + y) * LH + h, nzp = (zp * L + y) * LH + h;
 
-                        uint4 cv = Sc[n];
-                        const uint4 a0 = So[nxm], a1 = So[nxp], a2 = So[nym], a3 = So[nyp],
-                                    a4 = So[nzm], a5 = So[nzp];
+                        uint4 cv = ld4(Sc, n);
+                        const uint4 a0 = ld4(So, nxm), a1 = ld4(So, nxp), a2 = ld4(So, nym),
+                                    a3 = ld4(So, nyp), a4 = ld4(So, nzm), a5 = ld4(So, nzp);
                         const uint32_t f0 = __ldg(Fo + nxm), f1 = __ldg(Fc + n);
                         const uint32_t f2 = __ldg(Fo + N + nym), f3 = __ldg(Fc + N + n);
                         const uint32_t f4 = __ldg(Fo + 2 * N + nzm), f5 = __ldg(Fc + 2 * N + n);
@@ -410,7 +425,7 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
                                 wd[3] = cb ^ fl;
                             }
                         }
-                        Sc[n] = make_uint4(cw[0], cw[1], cw[2], cw[3]);
+                        st4(Sc, n, make_uint4(cw[0], cw[1], cw[2], cw[3]));
                     }
                     if constexpr (ACC) {
     #pragma unroll
@@ -452,7 +467,7 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int nn = n + u * TPQ;
-                    v[u] = nn < N ? Sq[nn] : make_uint4(0, 0, 0, 0);
+                    v[u] = nn < N ? ld4(Sq, nn) : make_uint4(0, 0, 0, 0);
                 }
                 vc_add4<NLD>(mc[0], v[0].x, v[1].x, v[2].x, v[3].x);
                 vc_add4<NLD>(mc[1], v[0].y, v[1].y, v[2].y, v[3].y);
@@ -543,63 +558,46 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
             }
             __syncthreads();
             // masked exchange of the accepted samples' configurations; on odd
-            // rounds the pair (3 of quad g, 0 of quad g+1) crosses quads, so
-            // each quad writes back only the words its own pairs touch
+            // rounds the pair (3 of quad g, 0 of quad g+1) crosses quads (and
+            // CTAs when g+1 lives in another CTA of the cluster)
             const uint32_t mA = sMask[2 * j], mB = sMask[2 * j + 1];
             // the mask words stay in sD: the thread that later reads word tid
             // of the overlap counts subtracts them again
             if (tid < 2 * Qc) mask_keep = sMask[tid];
+            // exchange the masked bits of two planes, chunks of 8 sites: all
+            // loads (some perhaps from a peer CTA) are in flight before the
+            // first store
+            auto exchange = [&](uint32_t* pa, uint32_t* pb, const uint32_t m) {
+                constexpr int CH = 8;
+                for (int n0 = lt; n0 < N; n0 += CH * TPQ) {
+                    uint32_t a[CH], b[CH];
+#pragma unroll
+                    for (int u = 0; u < CH; ++u) {
+                        const int n = n0 + u * TPQ;
+                        a[u] = n < N ? pa[n] : 0u;
+                        b[u] = n < N ? pb[n] : 0u;
+                    }
+#pragma unroll
+                    for (int u = 0; u < CH; ++u) {
+                        const int n = n0 + u * TPQ;
+                        if (n < N) {
+                            const uint32_t d = (a[u] ^ b[u]) & m;
+                            pa[n] = a[u] ^ d;
+                            pb[n] = b[u] ^ d;
+                        }
+                    }
+                }
+            };
             if (par == 0) {
-                if (mA | mB) {
-#pragma unroll 4
-                    for (int n = lt; n < N; n += TPQ) {
-                        uint4 v = Sq[n];
-                        const uint32_t d0 = (v.x ^ v.y) & mA;
-                        const uint32_t d1 = (v.z ^ v.w) & mB;
-                        v.x ^= d0;
-                        v.y ^= d0;
-                        v.z ^= d1;
-                        v.w ^= d1;
-                        Sq[n] = v;
-                    }
-                }
+                if (mA) exchange(Sq, Sq + N, mA);
+                if (mB) exchange(Sq + 2 * N, Sq + 3 * N, mB);
             } else {
-                if (mA) {
-                    uint32_t* base = reinterpret_cast<uint32_t*>(Sq);
-#pragma unroll 4
-                    for (int n = lt; n < N; n += TPQ) {
-                        const uint32_t y = base[4 * n + 1], z = base[4 * n + 2];
-                        const uint32_t d = (y ^ z) & mA;
-                        base[4 * n + 1] = y ^ d;
-                        base[4 * n + 2] = z ^ d;
-                    }
-                }
+                if (mA) exchange(Sq + N, Sq + 2 * N, mA);
                 if (mB) {
                     const int g2 = g + 1, r2 = g2 / Qc, j2 = g2 - r2 * Qc;
-                    uint32_t* nb = reinterpret_cast<uint32_t*>(
-                        cluster.map_shared_rank(S + (size_t)j2 * N, r2));
-                    uint32_t* base = reinterpret_cast<uint32_t*>(Sq);
-                    // chunks of 8 sites: all loads (some from the peer CTA) are in
-                    // flight together before the first store
-                    constexpr int CH = 8;
-                    for (int n0 = lt; n0 < N; n0 += CH * TPQ) {
-                        uint32_t a[CH], b[CH];
-#pragma unroll
-                        for (int u = 0; u < CH; ++u) {
-                            const int n = n0 + u * TPQ;
-                            a[u] = n < N ? base[4 * n + 3] : 0u;
-                            b[u] = n < N ? nb[4 * n] : 0u;
-                        }
-#pragma unroll
-                        for (int u = 0; u < CH; ++u) {
-                            const int n = n0 + u * TPQ;
-                            if (n < N) {
-                                const uint32_t d = (a[u] ^ b[u]) & mB;
-                                base[4 * n + 3] = a[u] ^ d;
-                                nb[4 * n] = b[u] ^ d;
-                            }
-                        }
-                    }
+                    uint32_t* nb = r2 == rank ? S + (size_t)j2 * 4 * N
+                                              : cluster.map_shared_rank(S + (size_t)j2 * 4 * N, r2);
+                    exchange(Sq + 3 * N, nb, mB);
                 }
             }
             cluster.sync();  // exchanges (local and remote) complete
@@ -629,8 +627,8 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
                 // the copy-0 quad's CTA.
                 const int gp = c == 0 ? g + Q : g - Q;
                 const int rp = gp / Qc, jp = gp - rp * Qc;
-                const uint4* Sp = cluster.map_shared_rank(S + (size_t)jp * N, rp);
-                const uint4* Sh = Sq + c * NH;
+                const uint32_t* Sp = cluster.map_shared_rank(S + (size_t)jp * 4 * N, rp);
+                const uint32_t* Sh = Sq + c * NH;
                 Sp += c * NH;
                 uint32_t dc[4][NLH];
 #pragma unroll
@@ -644,7 +642,7 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
                     for (int u = 0; u < 4; ++u) {
                         const int nn = n + u * TPQ;
                         if (nn < NH) {
-                            const uint4 a = Sh[nn], b = Sp[nn];
+                            const uint4 a = ld4(Sh, nn), b = ld4(Sp, nn);
                             v[u] = make_uint4(a.x ^ b.x, a.y ^ b.y, a.z ^ b.z, a.w ^ b.w);
                         } else {
                             v[u] = make_uint4(0, 0, 0, 0);
@@ -692,7 +690,10 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
     // ---- store this CTA's quads ----
     {
         uint4* dst = reinterpret_cast<uint4*>(P.spins) + qbase;
-        for (int i = tid; i < Qc * N; i += nthreads) dst[i] = S[i];
+        for (int i = tid; i < Qc * N; i += nthreads) {
+            const int jj = i / N, n = i - jj * N;
+            dst[i] = ld4(S + (size_t)jj * 4 * N, n);
+        }
     }
     cluster.sync();  // no CTA leaves while a peer may still read its shared memory
 }
