@@ -268,8 +268,8 @@ def run_ours(args, rank: int, world: int, dist) -> None:
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device=dev)  # 256 MiB > L2
 
     def step(k):
-        csg.run_device(cfg, spins.data_ptr(), bonds.data_ptr(), obs, SWEEP0 + k * SWEEPS_PER_STEP,
-                       SWEEPS_PER_STEP, stream.cuda_stream)
+        csg.run_device(cfg, spins.data_ptr(), bonds.data_ptr(), obs, SWEEP0 + k * args.sweeps_per_step,
+                       args.sweeps_per_step, stream.cuda_stream)
 
     for k in range(args.warmup):
         step(k)
@@ -296,7 +296,7 @@ def run_ours(args, rank: int, world: int, dist) -> None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_ms = float(t.item())
     boundary = int(acc["boundary"].item())
-    total_attempts = world * args.steps * SWEEPS_PER_STEP * attempts_per_sweep()
+    total_attempts = world * args.steps * args.sweeps_per_step * attempts_per_sweep()
     value = total_attempts / (t_ms * 1e6)
 
     # ---- end to end through the engine API: host state in, observables out ----
@@ -310,7 +310,7 @@ def run_ours(args, rank: int, world: int, dist) -> None:
     if rank != 0:
         return
     mean_launch_s = (sum(per_launch_ms) / len(per_launch_ms)) * 1e-3
-    word_updates = SWEEPS_PER_STEP * W * NCOPY * T * N
+    word_updates = args.sweeps_per_step * W * NCOPY * T * N
     achieved = word_updates * OPS_PER_WORD_UPDATE / mean_launch_s
     peak = int_peak_ops()
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
@@ -325,7 +325,7 @@ def run_ours(args, rank: int, world: int, dist) -> None:
             "e2e": {"value": e2e["value"], "unit": METRIC,
                     "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]},
             # resident kernel: one launch per 1024-sweep step; streaming engine: six per sweep
-            "gpu_launches": args.steps * (SWEEPS_PER_STEP * 6 if args.engine == "stream" else 1),
+            "gpu_launches": args.steps * (args.sweeps_per_step * 6 if args.engine == "stream" else 1),
             "exchange_boundary_cases": boundary,
             "clocks": clk.summary()}
     if world == 1 and not args.no_cpu_baseline:
@@ -349,19 +349,19 @@ def run_e2e(csg, torch, betas, seed, args, word0: int = 0) -> dict:
         hb[:] = b.ravel()
         spins_h, bonds_h = hs.reshape(s.shape), hb.reshape(b.shape)
         eng.set_state(spins_h, bonds_h, SWEEP0)
-        eng.run(SWEEPS_PER_STEP)
+        eng.run(args.sweeps_per_step)
         eng.observables()
         t0 = time.perf_counter()
         d2h = 0
         for k in range(args.steps):
-            eng.set_state(spins_h, bonds_h, SWEEP0 + k * SWEEPS_PER_STEP)
-            eng.run(SWEEPS_PER_STEP)
+            eng.set_state(spins_h, bonds_h, SWEEP0 + k * args.sweeps_per_step)
+            eng.run(args.sweeps_per_step)
             o = eng.observables()
             d2h = sum(getattr(o, f).nbytes for f in ("e_sum", "m_sum", "q_sum", "q2_sum", "q4_sum",
                                                      "hist", "e_last", "m_last", "d_last",
                                                      "swap_acc")) + 8
         el = time.perf_counter() - t0
-    attempts = args.steps * SWEEPS_PER_STEP * attempts_per_sweep()
+    attempts = args.steps * args.sweeps_per_step * attempts_per_sweep()
     return {"value": attempts / (el * 1e9), "seconds": el, "attempts": attempts,
             "h2d": int(hs.nbytes + hb.nbytes), "d2h": int(d2h)}
 
@@ -477,7 +477,8 @@ def run_large(args) -> None:
     peak = measured_hbm_peak()
     by_L = {}
     clk_summary = None
-    for (L_, W_, T_) in LARGE:
+    sizes = [c for c in LARGE if args.large_L in (None, c[0])]
+    for (L_, W_, T_) in sizes:
         N = L_ ** 3
         betas = 1.0 / (LARGE_T[0] * (LARGE_T[1] / LARGE_T[0]) ** (np.arange(T_) / (T_ - 1)))
         cfg, _k1 = csg.make_config(L_, W_, NCOPY, betas, seed=SEED, sweeps_per_swap=1,
@@ -504,7 +505,7 @@ def run_large(args) -> None:
             sweep += n
 
         for _ in range(args.warmup):
-            run(cfg, LARGE_SWEEPS_PER_STEP)
+            run(cfg, args.sweeps_per_step)
         torch.cuda.synchronize(dev)
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(args.steps)]
@@ -512,11 +513,11 @@ def run_large(args) -> None:
             for k in range(args.steps):
                 flush.fill_(k)
                 ev[k][0].record(stream)
-                run(cfg, LARGE_SWEEPS_PER_STEP)
+                run(cfg, args.sweeps_per_step)
                 ev[k][1].record(stream)
             torch.cuda.synchronize(dev)
         t_ms = sum(a.elapsed_time(b) for a, b in ev)
-        if L_ == LARGE[-1][0]:
+        if L_ == sizes[-1][0]:
             clk_summary = clk.summary()
         # colour kernel alone: Metropolis-only sweeps (two colour launches each)
         n_metro = 64
@@ -528,38 +529,52 @@ def run_large(args) -> None:
         b.record(stream)
         torch.cuda.synchronize(dev)
         colour_s = a.elapsed_time(b) * 1e-3 / (2 * n_metro)
-        quads = W_ * NCOPY * T_ // 4
-        colour_bytes = quads * (N // 2) * 16 * 3 + W_ * 3 * N * 4
         per_sweep = N * 32 * W_ * NCOPY * T_
-        by_L[L_] = {"attempts_per_ns": args.steps * LARGE_SWEEPS_PER_STEP * per_sweep / (t_ms * 1e6),
+        # per colour launch: half a sweep's attempts; 1.47 int ops and
+        # (8 + 12/(2 n_T))/32 HBM bytes per attempt (one pass per sweep)
+        launch_att = per_sweep / 2
+        colour_ops = launch_att * OPS_PER_WORD_UPDATE / 32
+        colour_bytes = launch_att * (8 + 12 / (2 * T_)) / 32
+        by_L[L_] = {"attempts_per_ns": args.steps * args.sweeps_per_step * per_sweep / (t_ms * 1e6),
                     "ms_per_step": t_ms / args.steps,
-                    "us_per_sweep": t_ms * 1e3 / (args.steps * LARGE_SWEEPS_PER_STEP),
+                    "us_per_sweep": t_ms * 1e3 / (args.steps * args.sweeps_per_step),
                     "spin_bytes": W_ * NCOPY * T_ * N * 4,
                     "metropolis_attempts_per_ns": per_sweep / (2 * colour_s * 1e9),
                     "colour_kernel": {"us_per_launch": colour_s * 1e6,
                                       "algorithmic_bytes_per_launch": colour_bytes,
-                                      "achieved_gbs": colour_bytes / colour_s / 1e9},
+                                      "achieved_gbs": colour_bytes / colour_s / 1e9,
+                                      "algorithmic_int_ops_per_launch": colour_ops,
+                                      "achieved_int_tops": colour_ops / colour_s / 1e12},
                     "exchange_boundary_cases": int(acc["boundary"].item())}
         del spins, bonds, acc
-    big = by_L[LARGE[-1][0]]
+    big = by_L[sizes[-1][0]]
+    ipeak = int_peak_ops()
     ck = big["colour_kernel"]
     line = {"metric": METRIC, "value": big["attempts_per_ns"], "unit": METRIC, "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": big["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic (seeded +-J disorder, uniform random initial spins)",
-            "config": {"workload": "large L, streaming engine (L=48; L=32 beside it)",
-                       "L": LARGE[-1][0], "samples": 32 * LARGE[-1][1], "copies": NCOPY,
-                       "temperatures": LARGE[-1][2], "T_range": list(LARGE_T),
-                       "sweeps_per_step": LARGE_SWEEPS_PER_STEP, "swap_every": 1,
+            "config": {"workload": "large L, streaming engine (L=" + str(sizes[-1][0]) +
+                                   ("; L=32 beside it)" if len(sizes) > 1 else ")"),
+                       "L": sizes[-1][0], "samples": 32 * sizes[-1][1], "copies": NCOPY,
+                       "temperatures": sizes[-1][2], "T_range": list(LARGE_T),
+                       "sweeps_per_step": args.sweeps_per_step, "swap_every": 1,
                        "measure_every": 1, "l2": "flushed between timed steps (256 MiB write); "
                        "the L=48 state (227 MB) is larger than L2"},
-            "roofline": {"bound": "hbm", "achieved": ck["achieved_gbs"], "peak": peak["gbs"],
-                         "unit": "GB/s", "frac": ck["achieved_gbs"] / peak["gbs"],
+            # the colour kernel's ideal time is set by its integer work (1.47 ops
+            # per attempt) more than by its HBM bytes (0.2559 B per attempt), so
+            # the integer pipe is its bound; the HBM fraction is given beside it
+            "roofline": {"bound": "int", "achieved": ck["achieved_int_tops"],
+                         "peak": ipeak["ops_per_s"] / 1e12, "unit": "Tops/s (32-bit integer logic)",
+                         "frac": ck["achieved_int_tops"] * 1e12 / ipeak["ops_per_s"],
                          "traffic": None, "kernel": "stream_colour_kernel (Metropolis only)",
-                         "peak_source": peak["source"]},
+                         "peak_source": ipeak["source"],
+                         "hbm": {"achieved": ck["achieved_gbs"], "peak": peak["gbs"], "unit": "GB/s",
+                                 "frac": ck["achieved_gbs"] / peak["gbs"],
+                                 "peak_source": peak["source"]}},
             "by_L": by_L,
             # per sweep: 2 colour launches, exchange decisions, exchange, overlap, measurement
-            "gpu_launches": args.steps * LARGE_SWEEPS_PER_STEP * 6, "clocks": clk_summary}
+            "gpu_launches": args.steps * args.sweeps_per_step * 6, "clocks": clk_summary}
     print(json.dumps(line), flush=True)
 
 
@@ -641,6 +656,10 @@ def main() -> None:
     ap.add_argument("--serve-budget-gb", type=float, default=16.0)
     ap.add_argument("--serve-slots", type=int, default=32)
     ap.add_argument("--serve-seed", type=int, default=5)
+    ap.add_argument("--sweeps-per-step", type=int, default=None,
+                    help="sweeps per timed step (default 1024; large workload 256)")
+    ap.add_argument("--large-L", type=int, choices=[32, 48], default=None,
+                    help="large workload: one lattice size only")
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the end-to-end leg (profiling runs)")
     args = ap.parse_args()
@@ -650,6 +669,8 @@ def main() -> None:
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
+    if args.sweeps_per_step is None:
+        args.sweeps_per_step = LARGE_SWEEPS_PER_STEP if args.workload == "large" else SWEEPS_PER_STEP
     if args.workload != "mixed":
         args.swap_every = 1 if args.swap_every is None else args.swap_every
         args.measure_every = 1 if args.measure_every is None else args.measure_every
