@@ -324,8 +324,8 @@ def run_ours(args, rank: int, world: int, dist) -> None:
                          "ops_per_attempt": OPS_PER_WORD_UPDATE / 32, "peak_source": peak["source"]},
             "e2e": {"value": e2e["value"], "unit": METRIC,
                     "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]},
-            # resident kernel: one launch per 1024-sweep step; streaming engine: six per sweep
-            "gpu_launches": args.steps * (args.sweeps_per_step * 6 if args.engine == "stream" else 1),
+            # resident kernel: one launch per 1024-sweep step; streaming engine: five per sweep
+            "gpu_launches": args.steps * (args.sweeps_per_step * 5 if args.engine == "stream" else 1),
             "exchange_boundary_cases": boundary,
             "clocks": clk.summary()}
     if world == 1 and not args.no_cpu_baseline:
@@ -573,8 +573,8 @@ def run_large(args) -> None:
                                  "frac": ck["achieved_gbs"] / peak["gbs"],
                                  "peak_source": peak["source"]}},
             "by_L": by_L,
-            # per sweep: 2 colour launches, exchange decisions, exchange, overlap, measurement
-            "gpu_launches": args.steps * args.sweeps_per_step * 6, "clocks": clk_summary}
+            # per sweep: 2 colour launches, exchange decisions, exchange with overlap, measurement
+            "gpu_launches": args.steps * args.sweeps_per_step * 5, "clocks": clk_summary}
     print(json.dumps(line), flush=True)
 
 

@@ -349,6 +349,9 @@ int run_stream(const csg_config& cfg, uint32_t* spins, const uint32_t* bonds,
     S.k1 = tp.k1;
     S.word0 = tp.word0;
     S.H = tp.H;
+    auto magic = [](uint64_t d) { return (uint32_t)(((uint64_t)1 << 32) / d + ((((uint64_t)1 << 32) % d) ? 1 : 0)); };
+    S.mag_plane = magic((uint64_t)d.L * (d.L / 2));
+    S.mag_row = magic((uint64_t)(d.L / 2));
     S.tab = tp.tab;
     csg::StreamObs O{};
     unsigned long long *boundary = nullptr, *swap_acc = nullptr;
@@ -400,11 +403,15 @@ int run_stream(const csg_config& cfg, uint32_t* spins, const uint32_t* bonds,
             csg::stream_decide_kernel<<<W * C, 256, 0, st>>>(S, s, par, need_M, do_swap, boundary,
                                                               swap_acc, swap_log, round - round0,
                                                               log_rounds);
-            if (do_swap) csg::stream_exchange_kernel<<<g_exchange, 256, 0, st>>>(S, par);
-            if (do_meas && obs) {
-                if (C == 2) csg::stream_overlap_kernel<<<g_overlap, csg::kStreamThreads, 0, st>>>(S);
-                csg::stream_measure_kernel<<<W, 256, 0, st>>>(S, need_M, O);
-            }
+            const bool overlap = do_meas && obs && C == 2;
+            if (do_swap && overlap)  // one pass: exchange, then count the overlaps
+                csg::stream_exchange_overlap_kernel<<<dim3(W, (unsigned)lay.nblk2), csg::kStreamThreads, 0,
+                                                      st>>>(S, par);
+            else if (do_swap)
+                csg::stream_exchange_kernel<<<g_exchange, 256, 0, st>>>(S, par);
+            else if (overlap)
+                csg::stream_overlap_kernel<<<g_overlap, csg::kStreamThreads, 0, st>>>(S);
+            if (do_meas && obs) csg::stream_measure_kernel<<<W * (unsigned)d.n_temps, 64, 0, st>>>(S, need_M, O);
         }
         ce = cudaGetLastError();
     }

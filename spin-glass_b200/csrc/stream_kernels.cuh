@@ -36,9 +36,19 @@ struct StreamParams {
     int nblk;   // blocks per quad and colour
     int nblk2;  // blocks per quad for the overlap (over all N sites)
     uint32_t k0, k1, word0;
+    uint32_t mag_plane;  // ceil(2^32 / (L*L/2)): division by multiply-high
+    uint32_t mag_row;    // ceil(2^32 / (L/2))
     double H;
     PtTables tab;
 };
+
+// n / d for 0 <= n < L^3/2, d in {L/2, L*L/2}, with mag = ceil(2^32 / d): the
+// multiply-high estimate is never below n / d and at most one above it for
+// every even L <= 128 (checked exhaustively), so one correction makes it exact.
+__device__ __forceinline__ int div_magic(int n, int d, uint32_t mag) {
+    const int q = (int)__umulhi((uint32_t)n, mag);
+    return q - (q * d > n ? 1 : 0);
+}
 
 // Measurement accumulators (layouts as in PtParams / csg_device_obs).
 struct StreamObs {
@@ -53,15 +63,6 @@ struct StreamObs {
     int* d_last;
 };
 
-__device__ __forceinline__ void site_coords(int n, int L, int& x, int& y, int& z, int p) {
-    const int LH = L / 2;
-    z = n / (L * LH);
-    const int rem = n - z * (L * LH);
-    y = rem / LH;
-    const int h = rem - y * LH;
-    x = 2 * h + ((y + z + p) & 1);
-}
-
 // One colour of one sweep.  blockIdx.x = quad (w, c, q), blockIdx.y = block
 // of kStreamSitesPerBlock sites of that colour; each thread updates
 // kStreamSPT sites in the 4 planes of the quad.  Consecutive blocks take the
@@ -71,7 +72,7 @@ template <bool GEN_H, bool ACC_E, bool ACC_M>
 __global__ void __launch_bounds__(kStreamThreads) stream_colour_kernel(const __grid_constant__ StreamParams P,
                                                                        int p, long long s) {
     const int L = P.L, LH = L / 2;
-    const long N = (long)L * L * L, NH = N / 2;
+    const int N = L * L * L, NH = N / 2;
     const int gq = blockIdx.x;
     const int w = gq / (P.C * P.Q), c = (gq / P.Q) % P.C, q = gq % P.Q;
     uint4* Sq = reinterpret_cast<uint4*>(P.spins) + (size_t)gq * N;
@@ -101,68 +102,57 @@ __global__ void __launch_bounds__(kStreamThreads) stream_colour_kernel(const __g
 #pragma unroll
         for (int l = 0; l < NLM; ++l) mcnt[k][l] = 0;
     }
-    const long n_base = (long)blockIdx.y * kStreamSitesPerBlock + threadIdx.x;
+    const int PL = L * LH;  // sites of one colour in one z plane
+    const int n_base = blockIdx.y * kStreamSitesPerBlock + threadIdx.x;
 #pragma unroll 1
     for (int m = 0; m < kStreamSPT; ++m) {
-        const long n = n_base + (long)m * kStreamThreads;
-        uint32_t wd[4][4] = {};
-        uint32_t up[4] = {0, 0, 0, 0};
-        if (n < NH) {
-            int x, y, z;
-            site_coords((int)n, L, x, y, z, p);
-            const int h = x >> 1, o = x & 1;
-            const int hxm = o ? h : (h == 0 ? LH - 1 : h - 1);
-            const int hxp = o ? (h == LH - 1 ? 0 : h + 1) : h;
-            const int ym = y == 0 ? L - 1 : y - 1, yp = y == L - 1 ? 0 : y + 1;
-            const int zm = z == 0 ? L - 1 : z - 1, zp = z == L - 1 ? 0 : z + 1;
-            const long row = ((long)z * L + y) * LH;
-            const long nxm = row + hxm, nxp = row + hxp;
-            const long nym = ((long)z * L + ym) * LH + h, nyp = ((long)z * L + yp) * LH + h;
-            const long nzm = ((long)zm * L + y) * LH + h, nzp = ((long)zp * L + y) * LH + h;
-            const uint4 cv = Sc[n];
-            const uint4 a0 = __ldg(So + nxm), a1 = __ldg(So + nxp), a2 = __ldg(So + nym),
-                        a3 = __ldg(So + nyp), a4 = __ldg(So + nzm), a5 = __ldg(So + nzp);
-            const uint32_t f0 = __ldg(Fo + nxm), f1 = __ldg(Fc + n);
-            const uint32_t f2 = __ldg(Fo + N + nym), f3 = __ldg(Fc + N + n);
-            const uint32_t f4 = __ldg(Fo + 2 * N + nzm), f5 = __ldg(Fc + 2 * N + n);
-            const u32x4 r = philox4x32_10((uint32_t)(((long)z * L + y) * L + x), (uint32_t)s, wg,
-                                          ctr3, P.k0, P.k1);
-            const uint32_t rr[4] = {r.v0, r.v1, r.v2, r.v3};
-            uint32_t cw[4] = {cv.x, cv.y, cv.z, cv.w};
-            const uint32_t n0w[4] = {a0.x, a0.y, a0.z, a0.w}, n1w[4] = {a1.x, a1.y, a1.z, a1.w};
-            const uint32_t n2w[4] = {a2.x, a2.y, a2.z, a2.w}, n3w[4] = {a3.x, a3.y, a3.z, a3.w};
-            const uint32_t n4w[4] = {a4.x, a4.y, a4.z, a4.w}, n5w[4] = {a5.x, a5.y, a5.z, a5.w};
+        const int n = n_base + m * kStreamThreads;
+        if (n >= (int)NH) break;  // n grows with m
+        // n = (z L + y) L/2 + h; divisions by multiply-high
+        const int z = div_magic(n, PL, P.mag_plane);
+        const int rem = n - z * PL;
+        const int y = div_magic(rem, LH, P.mag_row);
+        const int h = rem - y * LH;
+        const int o = (y + z + p) & 1;
+        const int x = 2 * h + o;
+        const int nxm = o ? n : (h == 0 ? n + LH - 1 : n - 1);
+        const int nxp = o ? (h == LH - 1 ? n - h : n + 1) : n;
+        const int nym = y == 0 ? n + PL - LH : n - LH;
+        const int nyp = y == L - 1 ? n - PL + LH : n + LH;
+        const int nzm = z == 0 ? n + (int)NH - PL : n - PL;
+        const int nzp = z == L - 1 ? n - (int)NH + PL : n + PL;
+        const uint4 cv = Sc[n];
+        const uint4 a0 = __ldg(So + nxm), a1 = __ldg(So + nxp), a2 = __ldg(So + nym),
+                    a3 = __ldg(So + nyp), a4 = __ldg(So + nzm), a5 = __ldg(So + nzp);
+        const uint32_t f0 = __ldg(Fo + nxm), f1 = __ldg(Fc + n);
+        const uint32_t f2 = __ldg(Fo + N + nym), f3 = __ldg(Fc + N + n);
+        const uint32_t f4 = __ldg(Fo + 2 * N + nzm), f5 = __ldg(Fc + 2 * N + n);
+        const u32x4 r = philox4x32_10((uint32_t)((z * L + y) * L + x), (uint32_t)s, wg, ctr3,
+                                      P.k0, P.k1);
+        const uint32_t rr[4] = {r.v0, r.v1, r.v2, r.v3};
+        uint32_t cw[4] = {cv.x, cv.y, cv.z, cv.w};
+        const uint32_t n0w[4] = {a0.x, a0.y, a0.z, a0.w}, n1w[4] = {a1.x, a1.y, a1.z, a1.w};
+        const uint32_t n2w[4] = {a2.x, a2.y, a2.z, a2.w}, n3w[4] = {a3.x, a3.y, a3.z, a3.w};
+        const uint32_t n4w[4] = {a4.x, a4.y, a4.z, a4.w}, n5w[4] = {a5.x, a5.y, a5.z, a5.w};
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const uint32_t s0 = cw[k];
-                const uint32_t u0 = s0 ^ n0w[k] ^ f0, u1 = s0 ^ n1w[k] ^ f1;
-                const uint32_t u2 = s0 ^ n2w[k] ^ f2, u3 = s0 ^ n3w[k] ^ f3;
-                const uint32_t u4 = s0 ^ n4w[k] ^ f4, u5 = s0 ^ n5w[k] ^ f5;
-                const uint32_t sa = u0 ^ u1 ^ u2, ca = maj3(u0, u1, u2);
-                const uint32_t sb = u3 ^ u4 ^ u5, cb = maj3(u3, u4, u5);
-                uint32_t fl;
-                if constexpr (GEN_H)
-                    fl = flip_gen(s0, sa, ca, sb, cb, rr[k], &P.tab.thr[4 * q + k][0][0],
-                                  &P.tab.ucut[4 * q + k][0]);
-                else
-                    fl = flip_h0(sa, ca, sb, cb, rr[k], th0[k], th1[k], th2[k]);
-                cw[k] = s0 ^ fl;
-                wd[k][0] = sa ^ fl;
-                wd[k][1] = sb ^ fl;
-                wd[k][2] = ca ^ fl;
-                wd[k][3] = cb ^ fl;
-                up[k] = cw[k];
-            }
-            Sc[n] = make_uint4(cw[0], cw[1], cw[2], cw[3]);
-        }
-        if constexpr (ACC_E) {
-#pragma unroll
-            for (int k = 0; k < 4; ++k) vc_add_site<NLV>(ecnt[k], wd[k][0], wd[k][1], wd[k][2], wd[k][3]);
-        }
-        if constexpr (ACC_M) {
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                uint32_t carry = up[k];
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t s0 = cw[k];
+            const uint32_t u0 = s0 ^ n0w[k] ^ f0, u1 = s0 ^ n1w[k] ^ f1;
+            const uint32_t u2 = s0 ^ n2w[k] ^ f2, u3 = s0 ^ n3w[k] ^ f3;
+            const uint32_t u4 = s0 ^ n4w[k] ^ f4, u5 = s0 ^ n5w[k] ^ f5;
+            const uint32_t sa = u0 ^ u1 ^ u2, ca = maj3(u0, u1, u2);
+            const uint32_t sb = u3 ^ u4 ^ u5, cb = maj3(u3, u4, u5);
+            uint32_t fl;
+            if constexpr (GEN_H)
+                fl = flip_gen(s0, sa, ca, sb, cb, rr[k], &P.tab.thr[4 * q + k][0][0],
+                              &P.tab.ucut[4 * q + k][0]);
+            else
+                fl = flip_h0(sa, ca, sb, cb, rr[k], th0[k], th1[k], th2[k]);
+            cw[k] = s0 ^ fl;
+            // post-flip unsatisfied bonds (energy) and spins up, counted at once
+            if constexpr (ACC_E) vc_add_site<NLV>(ecnt[k], sa ^ fl, sb ^ fl, ca ^ fl, cb ^ fl);
+            if constexpr (ACC_M) {
+                uint32_t carry = cw[k];
 #pragma unroll
                 for (int l = 0; l < NLM; ++l) {
                     const uint32_t t = mcnt[k][l] & carry;
@@ -171,6 +161,7 @@ __global__ void __launch_bounds__(kStreamThreads) stream_colour_kernel(const __g
                 }
             }
         }
+        Sc[n] = make_uint4(cw[0], cw[1], cw[2], cw[3]);
     }
     __shared__ int sred[2][4][32];
     if (ACC_E || ACC_M) {
@@ -292,6 +283,92 @@ __global__ void stream_exchange_kernel(const __grid_constant__ StreamParams P, i
     }
 }
 
+// Exchange and overlap in one pass (sweeps that both exchange and measure, two
+// copies): blockIdx.x = word, blockIdx.y = block of 2048 sites.  A thread takes
+// 4 sites of both copies and walks the quads in order; on odd rounds quad q is
+// final only after its pair (3 of q, 0 of q+1) is exchanged, so each quad is
+// written (and its overlap counted) one step after it is loaded.  Every word
+// is read and written by exactly one thread.  Partial overlap counts go to
+// d_part in the layout of stream_overlap_kernel.
+__global__ void __launch_bounds__(kStreamThreads) stream_exchange_overlap_kernel(
+    const __grid_constant__ StreamParams P, int par) {
+    constexpr int kSites = 4, kGroups = kStreamSitesPerBlock / (kStreamThreads * kSites);
+    const int N = P.L * P.L * P.L, T = P.T, Q = P.Q;
+    const int w = blockIdx.x, blk = blockIdx.y, lane = threadIdx.x & 31;
+    __shared__ int sD[kMaxT][32];
+    for (int i = threadIdx.x; i < T * 32; i += kStreamThreads) (&sD[0][0])[i] = 0;
+    __syncthreads();
+    uint4* base0 = reinterpret_cast<uint4*>(P.spins) + (size_t)(w * 2 + 0) * Q * N;
+    uint4* base1 = reinterpret_cast<uint4*>(P.spins) + (size_t)(w * 2 + 1) * Q * N;
+    const uint32_t* mk0 = P.masks + (size_t)(w * 2 + 0) * T;
+    const uint32_t* mk1 = P.masks + (size_t)(w * 2 + 1) * T;
+    for (int grp = 0; grp < kGroups; ++grp) {
+        int site[kSites];
+#pragma unroll
+        for (int i = 0; i < kSites; ++i)
+            site[i] = blk * kStreamSitesPerBlock + (grp * kSites + i) * kStreamThreads + threadIdx.x;
+        uint4 prv[2][kSites], cur[2][kSites];
+        // store quad qq and add its overlap counts
+        auto finish = [&](int qq, uint4 (&v)[2][kSites]) {
+            uint32_t x[4][kSites];
+#pragma unroll
+            for (int i = 0; i < kSites; ++i) {
+                if (site[i] < N) {
+                    base0[(size_t)qq * N + site[i]] = v[0][i];
+                    base1[(size_t)qq * N + site[i]] = v[1][i];
+                }
+                x[0][i] = v[0][i].x ^ v[1][i].x;
+                x[1][i] = v[0][i].y ^ v[1][i].y;
+                x[2][i] = v[0][i].z ^ v[1][i].z;
+                x[3][i] = v[0][i].w ^ v[1][i].w;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                uint32_t cnt[3] = {0, 0, 0};
+                vc_add4<3>(cnt, x[k][0], x[k][1], x[k][2], x[k][3]);
+                atomicAdd(&sD[4 * qq + k][lane], column_count<3>(cnt, lane));
+            }
+        };
+        for (int q = 0; q < Q; ++q) {
+            const uint32_t a0 = mk0[4 * q], a1 = mk0[4 * q + 1], a2 = mk0[4 * q + 2];
+            const uint32_t b0 = mk1[4 * q], b1 = mk1[4 * q + 1], b2 = mk1[4 * q + 2];
+#pragma unroll
+            for (int i = 0; i < kSites; ++i) {
+                const bool ok = site[i] < N;
+                uint4 u = ok ? base0[(size_t)q * N + site[i]] : make_uint4(0, 0, 0, 0);
+                uint4 v = ok ? base1[(size_t)q * N + site[i]] : make_uint4(0, 0, 0, 0);
+                if (par == 0) {  // (0,1) and (2,3) inside the quad
+                    uint32_t d = (u.x ^ u.y) & a0; u.x ^= d; u.y ^= d;
+                    d = (u.z ^ u.w) & a2; u.z ^= d; u.w ^= d;
+                    d = (v.x ^ v.y) & b0; v.x ^= d; v.y ^= d;
+                    d = (v.z ^ v.w) & b2; v.z ^= d; v.w ^= d;
+                } else {  // (1,2) inside; (3 of q-1, 0 of q) across
+                    uint32_t d = (u.y ^ u.z) & a1; u.y ^= d; u.z ^= d;
+                    d = (v.y ^ v.z) & b1; v.y ^= d; v.z ^= d;
+                    if (q > 0) {
+                        d = (prv[0][i].w ^ u.x) & mk0[4 * q - 1]; prv[0][i].w ^= d; u.x ^= d;
+                        d = (prv[1][i].w ^ v.x) & mk1[4 * q - 1]; prv[1][i].w ^= d; v.x ^= d;
+                    }
+                }
+                cur[0][i] = u;
+                cur[1][i] = v;
+            }
+            if (q > 0) finish(q - 1, prv);
+#pragma unroll
+            for (int i = 0; i < kSites; ++i) {
+                prv[0][i] = cur[0][i];
+                prv[1][i] = cur[1][i];
+            }
+        }
+        finish(Q - 1, prv);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < T * 32; i += kStreamThreads) {
+        const int t = i >> 5, b = i & 31;
+        P.d_part[((((size_t)w * Q + (t >> 2)) * P.nblk2 + blk) * 4 + (t & 3)) * 32 + b] = sD[t][b];
+    }
+}
+
 // Overlap partial sums: blockIdx.x = (w, q), blockIdx.y = block of sites;
 // each thread kStreamSPT sites.
 __global__ void __launch_bounds__(kStreamThreads) stream_overlap_kernel(const __grid_constant__ StreamParams P) {
@@ -339,12 +416,14 @@ __global__ void __launch_bounds__(kStreamThreads) stream_overlap_kernel(const __
 }
 
 // Measurement accumulators from the energies and the overlap partials:
-// block = w, thread = (t, sample).
+// blockIdx.x = (word, temperature), thread = (copy, sample); the first 32
+// threads also total the overlap partials of the plane.
 __global__ void stream_measure_kernel(const __grid_constant__ StreamParams P, bool need_M,
                                       StreamObs O) {
-    const int w = blockIdx.x, T = P.T, N = P.L * P.L * P.L;
-    for (int i = threadIdx.x; i < P.C * T * 32; i += blockDim.x) {
-        const size_t o = (size_t)w * P.C * T * 32 + i;
+    const int w = blockIdx.x / P.T, t = blockIdx.x % P.T, T = P.T, N = P.L * P.L * P.L;
+    const int c = threadIdx.x >> 5, b = threadIdx.x & 31;
+    if (c < P.C) {
+        const size_t o = (((size_t)w * P.C + c) * T + t) * 32 + b;
         const int e = P.energy[o], m = P.magn[o];
         if (O.e_sum) atomicAdd(reinterpret_cast<unsigned long long*>(O.e_sum + o), (unsigned long long)(long long)e);
         if (O.e_last) O.e_last[o] = e;
@@ -353,25 +432,24 @@ __global__ void stream_measure_kernel(const __grid_constant__ StreamParams P, bo
             if (O.m_last) O.m_last[o] = m;
         }
     }
-    if (P.C != 2) return;
-    for (int i = threadIdx.x; i < T * 32; i += blockDim.x) {
-        const int t = i >> 5, b = i & 31, q = t >> 2, k = t & 3;
-        int D = 0;
-        for (int blk = 0; blk < P.nblk2; ++blk)
-            D += P.d_part[((((size_t)(w * P.Q + q)) * P.nblk2 + blk) * 4 + k) * 32 + b];
-        const long long Qv = (long long)N - 2LL * D;
-        const unsigned long long q2 = (unsigned long long)(Qv * Qv);
-        const size_t o = ((size_t)w * T + t) * 32 + b;
-        if (O.q_sum) atomicAdd(reinterpret_cast<unsigned long long*>(O.q_sum + o), (unsigned long long)Qv);
-        if (O.q2_sum) atomicAdd(reinterpret_cast<unsigned long long*>(O.q2_sum + o), q2);
-        if (O.q4_sum) {
-            const unsigned long long lo = q2 * q2, hi = __umul64hi(q2, q2);
-            atomicAdd(O.q4_sum + 2 * o, lo & 0xFFFFFFFFull);
-            atomicAdd(O.q4_sum + 2 * o + 1, (lo >> 32) | (hi << 32));
-        }
-        if (O.hist) atomicAdd(&O.hist[(size_t)t * (N + 1) + D], 1u);
-        if (O.d_last) O.d_last[o] = D;
+    if (P.C != 2 || c != 0) return;
+    const int q = t >> 2, k = t & 3;
+    const int* dp = P.d_part + ((size_t)(w * P.Q + q) * P.nblk2 * 4 + k) * 32 + b;
+    int D = 0;
+#pragma unroll 4
+    for (int blk = 0; blk < P.nblk2; ++blk) D += dp[(size_t)blk * 128];
+    const long long Qv = (long long)N - 2LL * D;
+    const unsigned long long q2 = (unsigned long long)(Qv * Qv);
+    const size_t o = ((size_t)w * T + t) * 32 + b;
+    if (O.q_sum) atomicAdd(reinterpret_cast<unsigned long long*>(O.q_sum + o), (unsigned long long)Qv);
+    if (O.q2_sum) atomicAdd(reinterpret_cast<unsigned long long*>(O.q2_sum + o), q2);
+    if (O.q4_sum) {
+        const unsigned long long lo = q2 * q2, hi = __umul64hi(q2, q2);
+        atomicAdd(O.q4_sum + 2 * o, lo & 0xFFFFFFFFull);
+        atomicAdd(O.q4_sum + 2 * o + 1, (lo >> 32) | (hi << 32));
     }
+    if (O.hist) atomicAdd(&O.hist[(size_t)t * (N + 1) + D], 1u);
+    if (O.d_last) O.d_last[o] = D;
 }
 
 }  // namespace csg
