@@ -1146,9 +1146,10 @@ int csg_batch_set_plan(csg_batch* b, const int32_t* quads_per_cta) {
     return CSG_OK;
 }
 
-// Autotuner: coordinate descent over each member's quads per CTA, timing the
-// whole batch graph for probe_sweeps sweeps (best of two) with every other
-// member fixed; two passes.  The members' spins are saved before and restored
+// Autotuner: times the whole batch graph for probe_sweeps sweeps (best of two)
+// for every combination of the members' quads per CTA when there are at most
+// 256 combinations, otherwise coordinate descent over one member at a time
+// with the others fixed (two passes).  The members' spins are saved before and restored
 // after, and the probes accumulate no observables, so tuning leaves the
 // simulations exactly as they were.
 int csg_batch_tune(csg_batch* b, int64_t probe_sweeps, int32_t* chosen) {
@@ -1191,18 +1192,51 @@ int csg_batch_tune(csg_batch* b, int64_t probe_sweeps, int32_t* chosen) {
         rc = plan_member(b->eng[i], pl);  // start from the per-member plan
         if (rc == CSG_OK) b->eng[i]->qc = pl.Qc;
     }
-    for (int pass = 0; pass < 2 && rc == CSG_OK; ++pass)
+    // the quads-per-CTA values each member can take
+    std::vector<std::vector<int>> options(n);
+    size_t combos = 1;
+    for (size_t i = 0; i < n; ++i) {
+        csg_engine* e = b->eng[i];
+        const int G = e->cfg.dims.n_copies * e->cfg.dims.n_temps / 4;
+        const bool gen = e->cfg.H != 0.0;
+        const bool has_m = gen || (e->cfg.flags & CSG_MEASURE_M);
+        for (int qc = 1; qc <= G; ++qc)
+            if (G % qc == 0 && G / qc <= 16 && smem_for(e->cfg.dims.L, qc, has_m, gen) <= kMaxSmem &&
+                qc * csg::tpq_for(e->cfg.dims.L) <= csg::kMaxThreads)
+                options[i].push_back(qc);
+        combos *= std::max<size_t>(1, options[i].size());
+    }
+    if (combos <= 256) {
+        // few enough combinations: time every one (members share the GPU, so
+        // the best plan of one member depends on the others')
+        float best_ms = 1e30f;
+        std::vector<int> best(n), cur(n, 0);
+        for (size_t i = 0; i < n; ++i) best[i] = b->eng[i]->qc;
+        for (size_t k = 0; k < combos && rc == CSG_OK; ++k) {
+            size_t r = k;
+            for (size_t i = 0; i < n; ++i) {
+                const size_t m = options[i].size();
+                if (m) b->eng[i]->qc = options[i][r % m];
+                r /= std::max<size_t>(1, m);
+            }
+            float ms = 0.f;
+            if (time_batch(ms) != CSG_OK) {  // e.g. a cluster shape the device cannot place
+                cudaGetLastError();
+                continue;
+            }
+            if (ms < best_ms) {
+                best_ms = ms;
+                for (size_t i = 0; i < n; ++i) best[i] = b->eng[i]->qc;
+            }
+        }
+        for (size_t i = 0; i < n; ++i) b->eng[i]->qc = best[i];
+    }
+    for (int pass = 0; pass < 2 && rc == CSG_OK && combos > 256; ++pass)
         for (size_t i = 0; i < n && rc == CSG_OK; ++i) {
             csg_engine* e = b->eng[i];
-            const int G = e->cfg.dims.n_copies * e->cfg.dims.n_temps / 4;
-            const bool gen = e->cfg.H != 0.0;
-            const bool has_m = gen || (e->cfg.flags & CSG_MEASURE_M);
             int best_qc = e->qc;
             float best_ms = 1e30f;
-            for (int qc = 1; qc <= G && rc == CSG_OK; ++qc) {
-                if (G % qc || G / qc > 16 || smem_for(e->cfg.dims.L, qc, has_m, gen) > kMaxSmem ||
-                    qc * csg::tpq_for(e->cfg.dims.L) > csg::kMaxThreads)
-                    continue;
+            for (const int qc : options[i]) {
                 e->qc = qc;
                 float ms = 0.f;
                 const int r = time_batch(ms);

@@ -275,9 +275,12 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
     const int nthreads = blockDim.x;
     const int j = tid / TPQ;
     const int lt = tid - j * TPQ;
+    // Quad g of the word holds copy g % C and temperatures 4(g / C)..4(g / C)+3:
+    // the copies of one temperature quad sit side by side, so that with two
+    // copies most overlaps are counted from the CTA's own shared memory.
     const int g = rank * Qc + j;
-    const int c = g / Q;
-    const int q = g - c * Q;
+    const int c = g % C;
+    const int q = g / C;
     const int warp = tid >> 5, lane = tid & 31, nwarps = nthreads >> 5;
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -300,26 +303,30 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
     uint32_t* sThr = reinterpret_cast<uint32_t*>(sM + (has_M ? Qc * 4 * 32 : 0));
     uint8_t* sUcut = reinterpret_cast<uint8_t*>(sThr + Qc * 4 * 14);
 
-    // ---- load this CTA's quads (contiguous in global memory) ----
-    const size_t qbase = ((size_t)w * C * Q + (size_t)rank * Qc) * N;
+    // global offset of local quad jj (layout [W][C][T/4][N])
+    auto quad_base = [&](int jj) {
+        const int gg = rank * Qc + jj;
+        return ((size_t)(w * C + gg % C) * Q + gg / C) * N;
+    };
+    // ---- load this CTA's quads ----
     {
-        const uint4* src = reinterpret_cast<const uint4*>(P.spins) + qbase;
+        const uint4* src = reinterpret_cast<const uint4*>(P.spins);
         for (int i = tid; i < Qc * N; i += nthreads) {
             const int jj = i / N, n = i - jj * N;
-            st4(S + (size_t)jj * 4 * N, n, src[i]);
+            st4(S + (size_t)jj * 4 * N, n, src[quad_base(jj) + n]);
         }
     }
     if constexpr (GEN_H) {
         for (int i = tid; i < Qc * 4 * 14; i += nthreads) {
             const int pl = i / 14, k = i - pl * 14;
             const int gg = rank * Qc + pl / 4;
-            const int t = 4 * (gg % Q) + (pl & 3);
+            const int t = 4 * (gg / C) + (pl & 3);
             sThr[i] = P.tab.thr[t][k / 7][k % 7];
         }
         for (int i = tid; i < Qc * 4 * 2; i += nthreads) {
             const int pl = i / 2;
             const int gg = rank * Qc + pl / 4;
-            const int t = 4 * (gg % Q) + (pl & 3);
+            const int t = 4 * (gg / C) + (pl & 3);
             sUcut[i] = P.tab.ucut[t][i & 1];
         }
     }
@@ -495,7 +502,7 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
             // on the energies: draw it while the cluster barrier is pending
             auto uniform_for = [&](int pi) {
                 const int gg = rank * Qc + (pi >> 1);
-                const int cc = gg / Q, t = 4 * (gg - cc * Q) + par + 2 * (pi & 1);
+                const int cc = gg % C, t = 4 * (gg / C) + par + 2 * (pi & 1);
                 const u32x4 r = philox4x32_10((uint32_t)(lane >> 1), s32, wg,
                                               kTagSwap | ((uint32_t)cc << 8) | (uint32_t)t,
                                               P.k0, P.k1);
@@ -509,7 +516,7 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
                 const int jj = pi >> 1;
                 const int tq = par + 2 * (pi & 1);
                 const int gg = rank * Qc + jj;
-                const int cc = gg / Q, qq = gg - (gg / Q) * Q;
+                const int cc = gg % C, qq = gg / C;
                 const int t = 4 * qq + tq;
                 uint32_t mask = 0;
                 if (t + 1 < T) {
@@ -520,7 +527,7 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
                         E1 = E0 + 32;
                         M1 = M0 + 32;
                     } else {
-                        const int g2 = gg + 1, r2 = g2 / Qc, j2 = g2 - r2 * Qc;
+                        const int g2 = gg + C, r2 = g2 / Qc, j2 = g2 - r2 * Qc;  // next quad, same copy
                         E1 = cluster.map_shared_rank(sE + j2 * 4 * 32, r2);
                         M1 = cluster.map_shared_rank(sM + j2 * 4 * 32, r2);
                     }
@@ -594,7 +601,7 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
             } else {
                 if (mA) exchange(Sq + N, Sq + 2 * N, mA);
                 if (mB) {
-                    const int g2 = g + 1, r2 = g2 / Qc, j2 = g2 - r2 * Qc;
+                    const int g2 = g + C, r2 = g2 / Qc, j2 = g2 - r2 * Qc;  // next quad, same copy
                     uint32_t* nb = r2 == rank ? S + (size_t)j2 * 4 * N
                                               : cluster.map_shared_rank(S + (size_t)j2 * 4 * N, r2);
                     exchange(Sq + 3 * N, nb, mB);
@@ -609,7 +616,7 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
             for (int i = tid; i < Qc * 4 * 32; i += nthreads) {
                 const int pl = i >> 5, b = i & 31;
                 const int gg = rank * Qc + (pl >> 2);
-                const int cc = gg / Q, t = 4 * (gg - cc * Q) + (pl & 3);
+                const int cc = gg % C, t = 4 * (gg / C) + (pl & 3);
                 const size_t o = (((size_t)w * C + cc) * T + t) * 32 + b;
                 if (P.e_sum) atomicAdd(reinterpret_cast<unsigned long long*>(P.e_sum + o),
                                        (unsigned long long)(long long)sE[i]);
@@ -625,9 +632,10 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
                 // Overlap of quad q: the copy-0 team counts the colour-0 sites,
                 // the copy-1 team the colour-1 sites; both add into the counts of
                 // the copy-0 quad's CTA.
-                const int gp = c == 0 ? g + Q : g - Q;
+                const int gp = g ^ 1;  // the other copy's quad
                 const int rp = gp / Qc, jp = gp - rp * Qc;
-                const uint32_t* Sp = cluster.map_shared_rank(S + (size_t)jp * 4 * N, rp);
+                const uint32_t* Sp = rp == rank ? S + (size_t)jp * 4 * N
+                                                : cluster.map_shared_rank(S + (size_t)jp * 4 * N, rp);
                 const uint32_t* Sh = Sq + c * NH;
                 Sp += c * NH;
                 uint32_t dc[4][NLH];
@@ -653,7 +661,8 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
                     vc_add4<NLH>(dc[2], v[0].z, v[1].z, v[2].z, v[3].z);
                     vc_add4<NLH>(dc[3], v[0].w, v[1].w, v[2].w, v[3].w);
                 }
-                int* dst = c == 0 ? sD + j * 4 * 32 : cluster.map_shared_rank(sD + jp * 4 * 32, rp);
+                int* dst = c == 0 ? sD + j * 4 * 32
+                         : rp == rank ? sD + jp * 4 * 32 : cluster.map_shared_rank(sD + jp * 4 * 32, rp);
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     const int cnt = column_count<NLH>(dc[k], lane);
@@ -663,8 +672,8 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
                 for (int i = tid; i < Qc * 4 * 32; i += nthreads) {
                     const int pl = i >> 5, b = i & 31;
                     const int gg = rank * Qc + (pl >> 2);
-                    if (gg >= Q) continue;  // copy-1 quads: counted in the copy-0 owner
-                    const int t = 4 * gg + (pl & 3);
+                    if (gg & 1) continue;  // copy-1 quads: counted in the copy-0 owner
+                    const int t = 4 * (gg >> 1) + (pl & 3);
                     const int D = (int)((uint32_t)sD[i] - (i == tid ? mask_keep : 0u));
                     const long long Qv = (long long)N - 2LL * D;
                     const unsigned long long q2 = (unsigned long long)(Qv * Qv);
@@ -689,10 +698,10 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
 
     // ---- store this CTA's quads ----
     {
-        uint4* dst = reinterpret_cast<uint4*>(P.spins) + qbase;
+        uint4* dst = reinterpret_cast<uint4*>(P.spins);
         for (int i = tid; i < Qc * N; i += nthreads) {
             const int jj = i / N, n = i - jj * N;
-            dst[i] = ld4(S + (size_t)jj * 4 * N, n);
+            dst[quad_base(jj) + n] = ld4(S + (size_t)jj * 4 * N, n);
         }
     }
     cluster.sync();  // no CTA leaves while a peer may still read its shared memory
