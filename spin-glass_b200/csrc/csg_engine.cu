@@ -283,16 +283,17 @@ constexpr int64_t kSweepsPerLaunch = 1024;
 // sequence of one sweep.
 // ---------------------------------------------------------------------------
 struct StreamLayout {
-    int nblk = 0, nblk2 = 0;
+    int nblk = 0, nblk_plain = 0, nblk2 = 0;
     size_t e_part = 0, m_part = 0, d_part = 0, energy = 0, magn = 0, masks = 0, bytes = 0;
 };
 
 StreamLayout stream_layout(const csg_config& c) {
     const csg_dims& d = c.dims;
     const size_t N = (size_t)d.L * d.L * d.L, Q = (size_t)d.n_temps / 4;
-    const size_t spb = csg::kStreamSitesPerBlock;
+    const size_t spb = csg::kStreamSitesPerBlock, spa = csg::kStreamAccSitesPerBlock;
     StreamLayout s;
-    s.nblk = (int)((N / 2 + spb - 1) / spb);
+    s.nblk = (int)((N / 2 + spa - 1) / spa);  // blocks of the counting colour launches
+    s.nblk_plain = (int)((N / 2 + spb - 1) / spb);
     s.nblk2 = (int)((N + spb - 1) / spb);
     const size_t quads = (size_t)d.n_words * d.n_copies * Q;
     const size_t planes = (size_t)d.n_words * d.n_copies * d.n_temps;
@@ -308,11 +309,14 @@ StreamLayout stream_layout(const csg_config& c) {
     return s;
 }
 
-using ColourLaunch = void (*)(const csg::StreamParams&, dim3, int, long long, cudaStream_t);
+using ColourLaunch = void (*)(const csg::StreamParams&, const StreamLayout&, int, long long,
+                              cudaStream_t);
 
 template <bool G, bool E, bool M>
-void launch_colour(const csg::StreamParams& S, dim3 grid, int p, long long s, cudaStream_t st) {
-    csg::stream_colour_kernel<G, E, M><<<grid, csg::kStreamThreads, 0, st>>>(S, p, s);
+void launch_colour(const csg::StreamParams& S, const StreamLayout& lay, int p, long long s,
+                   cudaStream_t st) {
+    const dim3 grid((unsigned)(S.W * S.C * S.Q), (unsigned)(E || M ? lay.nblk : lay.nblk_plain));
+    csg::stream_colour_kernel<G, E, M><<<grid, csg::colour_threads<E || M>(), 0, st>>>(S, p, s);
 }
 
 ColourLaunch colour_launch(bool gen, bool acc_e, bool acc_m) {
@@ -384,7 +388,6 @@ int run_stream(const csg_config& cfg, uint32_t* spins, const uint32_t* bonds,
 
     const long N = (long)d.L * d.L * d.L;
     const unsigned W = (unsigned)d.n_words, C = (unsigned)d.n_copies, Q = (unsigned)S.Q;
-    const dim3 g_colour(W * C * Q, (unsigned)lay.nblk);
     const dim3 g_exchange(W * C, (unsigned)((N + 255) / 256));
     const dim3 g_overlap(W * Q, (unsigned)lay.nblk2);
     const int64_t sps = cfg.sched.sweeps_per_swap, spm = cfg.sched.sweeps_per_meas;
@@ -395,12 +398,13 @@ int run_stream(const csg_config& cfg, uint32_t* spins, const uint32_t* bonds,
         const bool do_meas = spm > 0 && (s + 1) % spm == 0 && s >= cfg.sched.meas_start;
         const bool need_E = do_swap || do_meas;
         const bool need_M = need_E && (gen || (do_meas && (cfg.flags & CSG_MEASURE_M)));
-        colour_launch(gen, false, need_M)(S, g_colour, 0, s, st);
-        colour_launch(gen, need_E, need_M)(S, g_colour, 1, s, st);
+        colour_launch(gen, false, need_M)(S, lay, 0, s, st);
+        colour_launch(gen, need_E, need_M)(S, lay, 1, s, st);
         if (need_E) {
             const long long round = do_swap ? (s + 1) / sps - 1 : 0;
             const int par = (int)(round & 1);
-            csg::stream_decide_kernel<<<W * C, 256, 0, st>>>(S, s, par, need_M, do_swap, boundary,
+            csg::stream_decide_kernel<<<W * C, std::min(1024, 32 * d.n_temps), 0, st>>>(
+                S, s, par, need_M, do_swap, boundary,
                                                               swap_acc, swap_log, round - round0,
                                                               log_rounds);
             const bool overlap = do_meas && obs && C == 2;

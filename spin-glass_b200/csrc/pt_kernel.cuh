@@ -511,7 +511,12 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
                 return (double)((((unsigned long long)hi << 32) | lo) >> 11) * 0x1p-53;
             };
             const double u_first = warp < 2 * Qc ? uniform_for(warp) : 0.0;
-            cluster.sync();  // energies of every plane of the word are visible
+            // Odd rounds pair plane 3 of a quad with plane 0 of the next, whose
+            // energies may live in another CTA; even rounds pair planes of one
+            // quad, so a CTA barrier suffices (the choice is the same in every
+            // CTA of the cluster).
+            if (par) cluster.sync();
+            else __syncthreads();
             for (int pi = warp; pi < 2 * Qc; pi += nwarps) {
                 const int jj = pi >> 1;
                 const int tq = par + 2 * (pi & 1);
@@ -607,7 +612,10 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
                     exchange(Sq + 3 * N, nb, mB);
                 }
             }
-            cluster.sync();  // exchanges (local and remote) complete
+            // exchanges (local and, on odd rounds, remote) complete; a
+            // measurement then reads the other copy's planes, perhaps remote
+            if (par || do_meas) cluster.sync();
+            else __syncthreads();
         } else {
             __syncthreads();
         }

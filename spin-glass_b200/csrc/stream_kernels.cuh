@@ -11,6 +11,7 @@
 // path) are reduced by the decision and measurement kernels.
 #pragma once
 #include <cstdint>
+#include <type_traits>
 
 #include "philox.cuh"
 #include "pt_kernel.cuh"
@@ -20,6 +21,13 @@ namespace csg {
 constexpr int kStreamThreads = 256;
 constexpr int kStreamSPT = 8;  // sites of one colour per thread per launch
 constexpr int kStreamSitesPerBlock = kStreamThreads * kStreamSPT;
+// Colour launches that count (energies, magnetisations) hold ~40 more
+// registers per thread; they run blocks of half the size so that more blocks
+// stay resident.  Their partial sums are per block of this many sites.
+constexpr int kStreamAccThreads = 128;
+constexpr int kStreamAccSitesPerBlock = kStreamAccThreads * kStreamSPT;
+template <bool ACC>
+__host__ __device__ constexpr int colour_threads() { return ACC ? kStreamAccThreads : kStreamThreads; }
 constexpr int kStreamNLV = bit_length(6 * kStreamSPT);  // bits of a per-thread bond count
 constexpr int kStreamNLM = bit_length(kStreamSPT);      // bits of a per-thread site count
 
@@ -64,12 +72,13 @@ struct StreamObs {
 };
 
 // One colour of one sweep.  blockIdx.x = quad (w, c, q), blockIdx.y = block
-// of kStreamSitesPerBlock sites of that colour; each thread updates
+// of kStreamSPT * blockDim.x sites of that colour; each thread updates
 // kStreamSPT sites in the 4 planes of the quad.  Consecutive blocks take the
 // quads of one word at the same sites, so the word's bonds are read once from
 // DRAM and then from L2.
 template <bool GEN_H, bool ACC_E, bool ACC_M>
-__global__ void __launch_bounds__(kStreamThreads) stream_colour_kernel(const __grid_constant__ StreamParams P,
+__global__ void __launch_bounds__(colour_threads<ACC_E || ACC_M>()) stream_colour_kernel(
+    const __grid_constant__ StreamParams P,
                                                                        int p, long long s) {
     const int L = P.L, LH = L / 2;
     const int N = L * L * L, NH = N / 2;
@@ -103,11 +112,10 @@ __global__ void __launch_bounds__(kStreamThreads) stream_colour_kernel(const __g
         for (int l = 0; l < NLM; ++l) mcnt[k][l] = 0;
     }
     const int PL = L * LH;  // sites of one colour in one z plane
-    const int n_base = blockIdx.y * kStreamSitesPerBlock + threadIdx.x;
-#pragma unroll 1
-    for (int m = 0; m < kStreamSPT; ++m) {
-        const int n = n_base + m * kStreamThreads;
-        if (n >= (int)NH) break;  // n grows with m
+    constexpr int BT = colour_threads<ACC_E || ACC_M>();
+    const int n_base = blockIdx.y * (BT * kStreamSPT) + threadIdx.x;
+    auto update_site = [&](const int n) {
+        if (n >= (int)NH) return;
         // n = (z L + y) L/2 + h; divisions by multiply-high
         const int z = div_magic(n, PL, P.mag_plane);
         const int rem = n - z * PL;
@@ -162,10 +170,14 @@ __global__ void __launch_bounds__(kStreamThreads) stream_colour_kernel(const __g
             }
         }
         Sc[n] = make_uint4(cw[0], cw[1], cw[2], cw[3]);
-    }
+    };
+    // one site at a time: two per iteration (more registers, fewer resident
+    // blocks) measured slower at L=48
+#pragma unroll 1
+    for (int m = 0; m < kStreamSPT; ++m) update_site(n_base + m * BT);
     __shared__ int sred[2][4][32];
     if (ACC_E || ACC_M) {
-        for (int i = threadIdx.x; i < 2 * 4 * 32; i += kStreamThreads) (&sred[0][0][0])[i] = 0;
+        for (int i = threadIdx.x; i < 2 * 4 * 32; i += BT) (&sred[0][0][0])[i] = 0;
         __syncthreads();
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
@@ -196,17 +208,20 @@ __global__ void stream_decide_kernel(const __grid_constant__ StreamParams P, lon
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     int* E = P.energy + (size_t)wc * T * 32;
     int* M = P.magn + (size_t)wc * T * 32;
-    for (int t = warp; t < T; t += nwarps) {
-        const int q = t >> 2, k = t & 3, gq = wc * P.Q + q;
+    // totals: one thread per (plane, sample), the partials of its plane's quad
+    for (int i = threadIdx.x; i < T * 32; i += blockDim.x) {
+        const int t = i >> 5, b = i & 31, q = t >> 2, k = t & 3, gq = wc * P.Q + q;
+        const int* ep = P.e_part + ((size_t)gq * P.nblk * 4 + k) * 32 + b;
         int u = 0, up = 0;
-        for (int b = 0; b < P.nblk; ++b) {
-            u += P.e_part[(((size_t)gq * P.nblk + b) * 4 + k) * 32 + lane];
-            if (need_M)
-                for (int pp = 0; pp < 2; ++pp)
-                    up += P.m_part[((((size_t)gq * 2 + pp) * P.nblk + b) * 4 + k) * 32 + lane];
+#pragma unroll 4
+        for (int blk = 0; blk < P.nblk; ++blk) u += ep[(size_t)blk * 128];
+        if (need_M) {
+            const int* mp = P.m_part + ((size_t)gq * 2 * P.nblk * 4 + k) * 32 + b;
+#pragma unroll 4
+            for (int blk = 0; blk < 2 * P.nblk; ++blk) up += mp[(size_t)blk * 128];
         }
-        E[t * 32 + lane] = 2 * u - 3 * N;
-        M[t * 32 + lane] = need_M ? 2 * up - N : 0;
+        E[i] = 2 * u - 3 * N;
+        M[i] = need_M ? 2 * up - N : 0;
     }
     __syncthreads();
     if (!do_swap) return;
