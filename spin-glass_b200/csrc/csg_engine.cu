@@ -1290,6 +1290,22 @@ size_t footprint_bytes(const csg_config& c) {
            (use_stream(c) ? stream_layout(c).bytes : 0);
 }
 
+// Quads per CTA for a request that shares the GPU with others: the largest
+// split that fits one CTA (fewest CTAs and cluster barriers per unit of work);
+// 0 (the single-request plan) for the streaming engine.
+int shared_gpu_qc(const csg_config& c) {
+    if (use_stream(c)) return 0;
+    const int G = c.dims.n_copies * c.dims.n_temps / 4;
+    const bool gen = !(c.H == 0.0);
+    const bool has_m = gen || (c.flags & CSG_MEASURE_M);
+    int best = 0;
+    for (int qc = 1; qc <= G; ++qc)
+        if (G % qc == 0 && G / qc <= 16 && smem_for(c.dims.L, qc, has_m, gen) <= kMaxSmem &&
+            qc * csg::tpq_for(c.dims.L) <= csg::kMaxThreads)
+            best = qc;
+    return best;
+}
+
 }  // namespace
 
 struct csg_server {
@@ -1388,10 +1404,15 @@ int csg_server_poll(csg_server* s, int64_t* completed, int32_t max_completed,
         s->active.back().cfg.betas = s->active.back().betas.data();
         s->active.back().e->cfg.betas = s->active.back().e->betas.data();
     }
+    int running = 0;
+    for (auto& r : s->active) running += (!r.done && r.launched < r.total) ? 1 : 0;
     for (auto& r : s->active) {
         if (r.done || r.launched >= r.total) continue;
         if (cudaStreamQuery(r.e->stream) != cudaSuccess) continue;
         const int64_t n = std::min<int64_t>(s->chunk, r.total - r.launched);
+        // alone, a request takes the plan that spreads it widest; sharing the
+        // GPU, the one with the fewest CTAs (every plan gives the same bits)
+        r.e->qc = running > 1 ? shared_gpu_qc(r.cfg) : 0;
         if (int rc = csg_run(r.e, n)) return rc;
         r.launched += n;
     }
