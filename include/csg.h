@@ -240,9 +240,10 @@ int csg_batch_run(csg_batch* b, int64_t n_sweeps);
 /* The same work as the plain engine would do it: member after member. */
 int csg_batch_run_sequential(csg_batch* b, int64_t n_sweeps);
 
-/* Autotuner: chooses each member's quads per CTA (hence its cluster size) by
- * timing the whole batch for probe_sweeps sweeps; states are restored after.
- * chosen (may be NULL) receives the choice per member. */
+/* Autotuner: chooses each member's quads per CTA (hence its cluster size), and
+ * whether every member CTA gets an SM of its own, by timing the whole batch
+ * for probe_sweeps sweeps; states are restored after.  chosen (may be NULL)
+ * receives the quads per CTA per member. */
 int csg_batch_tune(csg_batch* b, int64_t probe_sweeps, int32_t* chosen);
 
 /* Set each member's quads per CTA (0 = automatic). */

@@ -160,7 +160,8 @@ std::mutex g_plan_mu;
 csg_plan g_override = {0, 0, 0, 0};
 
 int prepare_kernel(KernelFn fn, size_t smem, int K) {
-    CSG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // the limit covers every plan of this kernel (several engines may share it)
+    CSG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
     // Ask for the smallest shared-memory carve-out that holds the CTA (plus the
     // 1 KB the system reserves per CTA) so that the rest of the SM's 256 KB
     // stays L1 for the bonds.
@@ -973,6 +974,9 @@ struct csg_batch {
     std::vector<cudaEvent_t> join;
     long long* counters = nullptr;  // device sweep counter per member
     std::vector<std::pair<int64_t, cudaGraphExec_t>> graphs;
+    // pad every member CTA's shared memory past half an SM, so that no two
+    // CTAs share an SM (chosen by the tuner)
+    bool spread = false;
 };
 
 namespace {
@@ -982,17 +986,25 @@ void drop_graphs(csg_batch* b) {
     b->graphs.clear();
 }
 
-int plan_member(csg_engine* e, Plan& pl) {
+// more than half of an SM's 228 KB (with the 1 KB per-CTA reserve)
+constexpr size_t kSpreadSmem = 116 * 1024;
+
+int plan_member(csg_engine* e, Plan& pl, bool spread = false) {
     csg::PtParams P;
     bool gen = false;
     fill_params(e->cfg, P, gen);
-    return make_plan(e->cfg, gen, pl, e->qc);
+    if (int rc = make_plan(e->cfg, gen, pl, e->qc)) return rc;
+    if (spread && pl.smem < kSpreadSmem) {
+        pl.smem = kSpreadSmem;
+        return prepare_kernel(select_kernel(e->cfg.dims.L, gen), pl.smem, pl.K);
+    }
+    return CSG_OK;
 }
 
 int capture(csg_batch* b, int64_t n_sweeps, bool with_obs, cudaGraphExec_t* out) {
     std::vector<Plan> plans(b->eng.size());
     for (size_t i = 0; i < b->eng.size(); ++i)
-        if (int rc = plan_member(b->eng[i], plans[i])) return rc;
+        if (int rc = plan_member(b->eng[i], plans[i], b->spread)) return rc;
     CSG_CUDA(cudaStreamBeginCapture(b->main, cudaStreamCaptureModeThreadLocal));
     int rc = CSG_OK;
     cudaError_t ce = cudaEventRecord(b->fork, b->main);
@@ -1151,8 +1163,9 @@ int csg_batch_set_plan(csg_batch* b, const int32_t* quads_per_cta) {
 }
 
 // Autotuner: times the whole batch graph for probe_sweeps sweeps (best of two)
-// for every combination of the members' quads per CTA when there are at most
-// 256 combinations, otherwise coordinate descent over one member at a time
+// for every combination of the members' quads per CTA, each with and without
+// one SM per CTA, when there are at most 256 such combinations; otherwise
+// coordinate descent over one member at a time
 // with the others fixed (two passes).  The members' spins are saved before and restored
 // after, and the probes accumulate no observables, so tuning leaves the
 // simulations exactly as they were.
@@ -1210,14 +1223,17 @@ int csg_batch_tune(csg_batch* b, int64_t probe_sweeps, int32_t* chosen) {
                 options[i].push_back(qc);
         combos *= std::max<size_t>(1, options[i].size());
     }
-    if (combos <= 256) {
-        // few enough combinations: time every one (members share the GPU, so
-        // the best plan of one member depends on the others')
+    if (2 * combos <= 256) {
+        // few enough combinations: time every one, with and without one SM per
+        // CTA (members share the GPU, so the best plan of one member depends
+        // on the others')
         float best_ms = 1e30f;
-        std::vector<int> best(n), cur(n, 0);
+        bool best_spread = false;
+        std::vector<int> best(n);
         for (size_t i = 0; i < n; ++i) best[i] = b->eng[i]->qc;
-        for (size_t k = 0; k < combos && rc == CSG_OK; ++k) {
-            size_t r = k;
+        for (size_t k = 0; k < 2 * combos && rc == CSG_OK; ++k) {
+            b->spread = k >= combos;
+            size_t r = k % combos;
             for (size_t i = 0; i < n; ++i) {
                 const size_t m = options[i].size();
                 if (m) b->eng[i]->qc = options[i][r % m];
@@ -1230,12 +1246,14 @@ int csg_batch_tune(csg_batch* b, int64_t probe_sweeps, int32_t* chosen) {
             }
             if (ms < best_ms) {
                 best_ms = ms;
+                best_spread = b->spread;
                 for (size_t i = 0; i < n; ++i) best[i] = b->eng[i]->qc;
             }
         }
         for (size_t i = 0; i < n; ++i) b->eng[i]->qc = best[i];
+        b->spread = best_spread;
     }
-    for (int pass = 0; pass < 2 && rc == CSG_OK && combos > 256; ++pass)
+    for (int pass = 0; pass < 2 && rc == CSG_OK && 2 * combos > 256; ++pass)
         for (size_t i = 0; i < n && rc == CSG_OK; ++i) {
             csg_engine* e = b->eng[i];
             int best_qc = e->qc;
