@@ -284,26 +284,16 @@ constexpr int64_t kSweepsPerLaunch = 1024;
 // sequence of one sweep.
 // ---------------------------------------------------------------------------
 struct StreamLayout {
-    bool staged = false;  // colour launches with planes staged in shared memory
     int nblk = 0, nblk_plain = 0, nblk2 = 0;
-    size_t e_part = 0, m_part = 0, d_part = 0, energy = 0, magn = 0, masks = 0, err = 0, bytes = 0;
+    size_t e_part = 0, m_part = 0, d_part = 0, energy = 0, magn = 0, masks = 0, bytes = 0;
 };
 
-// The staged colour kernel holds 4 z-planes of one quad's colour halves in
-// shared memory (4 * L*L/2 * 16 bytes: 131 KB at L = 64), used for L = 32..64;
-// its bulk copies need the spins 16-byte aligned.
-bool staged_ok(int L, const void* spins) {
-    return L >= 32 && L <= 64 && ((uintptr_t)spins & 15) == 0;
-}
-
-StreamLayout stream_layout(const csg_config& c, bool staged) {
+StreamLayout stream_layout(const csg_config& c) {
     const csg_dims& d = c.dims;
     const size_t N = (size_t)d.L * d.L * d.L, Q = (size_t)d.n_temps / 4;
     const size_t spb = csg::kStreamSitesPerBlock, spa = csg::kStreamAccSitesPerBlock;
     StreamLayout s;
-    s.staged = staged;
-    // blocks per quad of the colour launches that write partial sums
-    s.nblk = staged ? d.L : (int)((N / 2 + spa - 1) / spa);
+    s.nblk = (int)((N / 2 + spa - 1) / spa);  // blocks of the counting colour launches
     s.nblk_plain = (int)((N / 2 + spb - 1) / spb);
     s.nblk2 = (int)((N + spb - 1) / spb);
     const size_t quads = (size_t)d.n_words * d.n_copies * Q;
@@ -316,13 +306,8 @@ StreamLayout stream_layout(const csg_config& c, bool staged) {
     s.energy = off, off += up(planes * 32 * 4);
     s.magn = off, off += up(planes * 32 * 4);
     s.masks = off, off += up(planes * 4);
-    s.err = off, off += 256;
     s.bytes = off;
     return s;
-}
-
-size_t stream_scratch_bytes(const csg_config& c) {
-    return std::max(stream_layout(c, false).bytes, stream_layout(c, true).bytes);
 }
 
 using ColourLaunch = void (*)(const csg::StreamParams&, const StreamLayout&, int, long long,
@@ -331,16 +316,6 @@ using ColourLaunch = void (*)(const csg::StreamParams&, const StreamLayout&, int
 template <bool G, bool E, bool M>
 void launch_colour(const csg::StreamParams& S, const StreamLayout& lay, int p, long long s,
                    cudaStream_t st) {
-    if (lay.staged) {
-        static const bool attr = cudaFuncSetAttribute(csg::stream_colour_staged_kernel<G, E, M>,
-                                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                      (int)csg::staged_smem_bytes(64)) == cudaSuccess;
-        (void)attr;  // a failure shows as a launch error below
-        const dim3 grid((unsigned)(S.W * S.C * S.Q), (unsigned)S.L);
-        csg::stream_colour_staged_kernel<G, E, M><<<grid, csg::kStreamThreads,
-                                                    csg::staged_smem_bytes(S.L), st>>>(S, p, s);
-        return;
-    }
     const dim3 grid((unsigned)(S.W * S.C * S.Q), (unsigned)(E || M ? lay.nblk : lay.nblk_plain));
     csg::stream_colour_kernel<G, E, M><<<grid, csg::colour_threads<E || M>(), 0, st>>>(S, p, s);
 }
@@ -363,7 +338,7 @@ int run_stream(const csg_config& cfg, uint32_t* spins, const uint32_t* bonds,
     bool gen = false;
     fill_params(cfg, tp, gen);
     const csg_dims& d = cfg.dims;
-    const StreamLayout lay = stream_layout(cfg, staged_ok(d.L, spins));
+    const StreamLayout lay = stream_layout(cfg);
     csg::StreamParams S;
     std::memset(&S, 0, sizeof(S));
     S.spins = spins;
@@ -411,8 +386,6 @@ int run_stream(const csg_config& cfg, uint32_t* spins, const uint32_t* bonds,
     S.energy = reinterpret_cast<int*>(base + lay.energy);
     S.magn = reinterpret_cast<int*>(base + lay.magn);
     S.masks = reinterpret_cast<uint32_t*>(base + lay.masks);
-    S.err = reinterpret_cast<int*>(base + lay.err);
-    CSG_CUDA(cudaMemsetAsync(S.err, 0, sizeof(int), st));
 
     const long N = (long)d.L * d.L * d.L;
     const unsigned W = (unsigned)d.n_words, C = (unsigned)d.n_copies, Q = (unsigned)S.Q;
@@ -447,16 +420,9 @@ int run_stream(const csg_config& cfg, uint32_t* spins, const uint32_t* bonds,
         }
         ce = cudaGetLastError();
     }
-    // the staged launches report a shared-memory staging wait that gave up
-    int err = 0;
-    if (ce == cudaSuccess && lay.staged) {
-        ce = cudaMemcpyAsync(&err, S.err, sizeof(int), cudaMemcpyDeviceToHost, st);
-        if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
-    }
     const cudaError_t ce2 = cudaFreeAsync(base, st);
     if (ce != cudaSuccess) return fail(CSG_ERR_CUDA, std::string("stream launch: ") + cudaGetErrorString(ce));
     if (ce2 != cudaSuccess) return fail(CSG_ERR_CUDA, std::string("cudaFreeAsync: ") + cudaGetErrorString(ce2));
-    if (err) return fail(CSG_ERR_CUDA, "streaming engine: a shared-memory staging wait timed out");
     return CSG_OK;
 }
 
@@ -1339,7 +1305,7 @@ size_t footprint_bytes(const csg_config& c) {
     return (size_t)d.n_words * d.n_copies * d.n_temps * N * 4 + (size_t)d.n_words * 3 * N * 4 +
            ne * (8 + 8 + 4 + 4) + nq * (8 + 8 + 16 + 4) + nh * 4 +
            (size_t)d.n_copies * d.n_temps * 8 + (size_t)c.swap_log_rounds * ne / 32 * 4 + 8 +
-           (use_stream(c) ? stream_scratch_bytes(c) : 0);
+           (use_stream(c) ? stream_layout(c).bytes : 0);
 }
 
 // Quads per CTA for a request that shares the GPU with others: the largest

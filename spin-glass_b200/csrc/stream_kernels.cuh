@@ -40,7 +40,6 @@ struct StreamParams {
     int* energy;  // [W][C][T][32] bond energies after the exchange
     int* magn;    // [W][C][T][32]
     uint32_t* masks;  // [W][C][T] accepted-sample masks of the current round
-    int* err;         // set to 1 when a shared-memory staging wait gives up
     int L, W, C, T, Q;
     int nblk;   // blocks per quad and colour
     int nblk2;  // blocks per quad for the overlap (over all N sites)
@@ -72,79 +71,6 @@ struct StreamObs {
     int* d_last;
 };
 
-// The update of one site in the 4 planes of quad q (the arithmetic of the
-// resident kernel's colour pass), with the post-flip unsatisfied bonds
-// (energy) and spins up (magnetisation) added to bit-sliced counters.
-template <bool GEN_H, bool ACC_E, bool ACC_M, int NLV, int NLM>
-__device__ __forceinline__ uint4 stream_site_update(const StreamParams& P, int q, const uint4 cv,
-                                                    const uint4 (&a)[6], const uint32_t (&f)[6],
-                                                    const u32x4 r, const uint32_t (&th0)[4],
-                                                    const uint32_t (&th1)[4],
-                                                    const uint32_t (&th2)[4],
-                                                    uint32_t (&ecnt)[4][NLV],
-                                                    uint32_t (&mcnt)[4][NLM]) {
-    const uint32_t rr[4] = {r.v0, r.v1, r.v2, r.v3};
-    uint32_t cw[4] = {cv.x, cv.y, cv.z, cv.w};
-    const uint32_t nw[6][4] = {{a[0].x, a[0].y, a[0].z, a[0].w}, {a[1].x, a[1].y, a[1].z, a[1].w},
-                               {a[2].x, a[2].y, a[2].z, a[2].w}, {a[3].x, a[3].y, a[3].z, a[3].w},
-                               {a[4].x, a[4].y, a[4].z, a[4].w}, {a[5].x, a[5].y, a[5].z, a[5].w}};
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const uint32_t s0 = cw[k];
-        const uint32_t u0 = s0 ^ nw[0][k] ^ f[0], u1 = s0 ^ nw[1][k] ^ f[1];
-        const uint32_t u2 = s0 ^ nw[2][k] ^ f[2], u3 = s0 ^ nw[3][k] ^ f[3];
-        const uint32_t u4 = s0 ^ nw[4][k] ^ f[4], u5 = s0 ^ nw[5][k] ^ f[5];
-        const uint32_t sa = u0 ^ u1 ^ u2, ca = maj3(u0, u1, u2);
-        const uint32_t sb = u3 ^ u4 ^ u5, cb = maj3(u3, u4, u5);
-        uint32_t fl;
-        if constexpr (GEN_H)
-            fl = flip_gen(s0, sa, ca, sb, cb, rr[k], &P.tab.thr[4 * q + k][0][0],
-                          &P.tab.ucut[4 * q + k][0]);
-        else
-            fl = flip_h0(sa, ca, sb, cb, rr[k], th0[k], th1[k], th2[k]);
-        cw[k] = s0 ^ fl;
-        if constexpr (ACC_E) vc_add_site<NLV>(ecnt[k], sa ^ fl, sb ^ fl, ca ^ fl, cb ^ fl);
-        if constexpr (ACC_M) {
-            uint32_t carry = cw[k];
-#pragma unroll
-            for (int l = 0; l < NLM; ++l) {
-                const uint32_t t = mcnt[k][l] & carry;
-                mcnt[k][l] ^= carry;
-                carry = t;
-            }
-        }
-    }
-    return make_uint4(cw[0], cw[1], cw[2], cw[3]);
-}
-
-// Per-block partial sums of the counters: e_part[gq][blockIdx.y][4][32] and
-// m_part[gq][colour][blockIdx.y][4][32] (blockDim.x >= 128).
-template <bool ACC_E, bool ACC_M, int NLV, int NLM>
-__device__ __forceinline__ void stream_store_partials(const StreamParams& P, int gq, int p,
-                                                      const uint32_t (&ecnt)[4][NLV],
-                                                      const uint32_t (&mcnt)[4][NLM]) {
-    if constexpr (ACC_E || ACC_M) {
-        __shared__ int sred[2][4][32];
-        const int lane = threadIdx.x & 31;
-        for (int i = threadIdx.x; i < 2 * 4 * 32; i += blockDim.x) (&sred[0][0][0])[i] = 0;
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            if constexpr (ACC_E) atomicAdd(&sred[0][k][lane], column_count<NLV>(ecnt[k], lane));
-            if constexpr (ACC_M) atomicAdd(&sred[1][k][lane], column_count<NLM>(mcnt[k], lane));
-        }
-        __syncthreads();
-        if (threadIdx.x < 128) {
-            const int k = threadIdx.x >> 5;
-            if constexpr (ACC_E)
-                P.e_part[(((size_t)gq * P.nblk + blockIdx.y) * 4 + k) * 32 + lane] = sred[0][k][lane];
-            if constexpr (ACC_M)
-                P.m_part[((((size_t)gq * 2 + p) * P.nblk + blockIdx.y) * 4 + k) * 32 + lane] =
-                    sred[1][k][lane];
-        }
-    }
-}
-
 // One colour of one sweep.  blockIdx.x = quad (w, c, q), blockIdx.y = block
 // of kStreamSPT * blockDim.x sites of that colour; each thread updates
 // kStreamSPT sites in the 4 planes of the quad.  Consecutive blocks take the
@@ -152,7 +78,8 @@ __device__ __forceinline__ void stream_store_partials(const StreamParams& P, int
 // DRAM and then from L2.
 template <bool GEN_H, bool ACC_E, bool ACC_M>
 __global__ void __launch_bounds__(colour_threads<ACC_E || ACC_M>()) stream_colour_kernel(
-    const __grid_constant__ StreamParams P, int p, long long s) {
+    const __grid_constant__ StreamParams P,
+                                                                       int p, long long s) {
     const int L = P.L, LH = L / 2;
     const int N = L * L * L, NH = N / 2;
     const int gq = blockIdx.x;
@@ -165,6 +92,7 @@ __global__ void __launch_bounds__(colour_threads<ACC_E || ACC_M>()) stream_colou
     const uint32_t* Fo = Fw + (1 - p) * NH;
     const uint32_t ctr3 = kTagSweep | ((uint32_t)c << 8) | (uint32_t)q;
     const uint32_t wg = (uint32_t)w + P.word0;
+    const int lane = threadIdx.x & 31;
     uint32_t th0[4], th1[4], th2[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -186,12 +114,8 @@ __global__ void __launch_bounds__(colour_threads<ACC_E || ACC_M>()) stream_colou
     const int PL = L * LH;  // sites of one colour in one z plane
     constexpr int BT = colour_threads<ACC_E || ACC_M>();
     const int n_base = blockIdx.y * (BT * kStreamSPT) + threadIdx.x;
-    // one site at a time: two per iteration (more registers, fewer resident
-    // blocks) measured slower at L=48
-#pragma unroll 1
-    for (int m = 0; m < kStreamSPT; ++m) {
-        const int n = n_base + m * BT;
-        if (n >= (int)NH) break;  // n grows with m
+    auto update_site = [&](const int n) {
+        if (n >= (int)NH) return;
         // n = (z L + y) L/2 + h; divisions by multiply-high
         const int z = div_magic(n, PL, P.mag_plane);
         const int rem = n - z * PL;
@@ -205,140 +129,71 @@ __global__ void __launch_bounds__(colour_threads<ACC_E || ACC_M>()) stream_colou
         const int nyp = y == L - 1 ? n - PL + LH : n + LH;
         const int nzm = z == 0 ? n + (int)NH - PL : n - PL;
         const int nzp = z == L - 1 ? n - (int)NH + PL : n + PL;
-        const uint4 a[6] = {__ldg(So + nxm), __ldg(So + nxp), __ldg(So + nym),
-                            __ldg(So + nyp), __ldg(So + nzm), __ldg(So + nzp)};
-        const uint32_t f[6] = {__ldg(Fo + nxm), __ldg(Fc + n), __ldg(Fo + N + nym),
-                               __ldg(Fc + N + n), __ldg(Fo + 2 * N + nzm), __ldg(Fc + 2 * N + n)};
+        const uint4 cv = Sc[n];
+        const uint4 a0 = __ldg(So + nxm), a1 = __ldg(So + nxp), a2 = __ldg(So + nym),
+                    a3 = __ldg(So + nyp), a4 = __ldg(So + nzm), a5 = __ldg(So + nzp);
+        const uint32_t f0 = __ldg(Fo + nxm), f1 = __ldg(Fc + n);
+        const uint32_t f2 = __ldg(Fo + N + nym), f3 = __ldg(Fc + N + n);
+        const uint32_t f4 = __ldg(Fo + 2 * N + nzm), f5 = __ldg(Fc + 2 * N + n);
         const u32x4 r = philox4x32_10((uint32_t)((z * L + y) * L + x), (uint32_t)s, wg, ctr3,
                                       P.k0, P.k1);
-        Sc[n] = stream_site_update<GEN_H, ACC_E, ACC_M, NLV, NLM>(P, q, Sc[n], a, f, r, th0, th1,
-                                                                  th2, ecnt, mcnt);
-    }
-    stream_store_partials<ACC_E, ACC_M, NLV, NLM>(P, gq, p, ecnt, mcnt);
-}
-
-// ---- bulk copies into shared memory (TMA, 1-D), completion on an mbarrier ----
-__device__ __forceinline__ uint32_t smem_u32(const void* ptr) {
-    return (uint32_t)__cvta_generic_to_shared(ptr);
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-// global -> shared, 16-byte aligned addresses, size a multiple of 16
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(bar))
-        : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-constexpr int kWaitTries = 1 << 22;  // bound on every mbarrier wait
-
-// Shared memory of the staged colour kernel: the block's own plane and the
-// other colour's planes z-1, z, z+1 (4 * L*L/2 uint4).
-__host__ __device__ inline size_t staged_smem_bytes(int L) { return (size_t)4 * L * (L / 2) * 16; }
-
-// One colour of one sweep with the planes staged in shared memory:
-// blockIdx.x = quad (w, c, q), blockIdx.y = z plane.  One thread issues four
-// bulk copies (own plane z; other colour's planes z-1, z, z+1), every thread
-// waits on the mbarrier (bounded), then updates sites of plane z from shared
-// memory and writes them back to global memory.  Same arithmetic, counters
-// and partial-sum layout (blocks per quad = L) as stream_colour_kernel.
-template <bool GEN_H, bool ACC_E, bool ACC_M>
-__global__ void __launch_bounds__(kStreamThreads) stream_colour_staged_kernel(
-    const __grid_constant__ StreamParams P, int p, long long s) {
-    const int L = P.L, LH = L / 2, PL = L * LH;
-    const int N = L * L * L, NH = N / 2;
-    const int gq = blockIdx.x, z = blockIdx.y;
-    const int w = gq / (P.C * P.Q), c = (gq / P.Q) % P.C, q = gq % P.Q;
-    uint4* Sq = reinterpret_cast<uint4*>(P.spins) + (size_t)gq * N;
-    uint4* Sc = Sq + p * NH;
-    const uint4* So = Sq + (1 - p) * NH;
-    const uint32_t* Fw = P.bonds + (size_t)w * 3 * N;
-    const uint32_t* Fc = Fw + p * NH;
-    const uint32_t* Fo = Fw + (1 - p) * NH;
-    const int zm = z == 0 ? L - 1 : z - 1, zp = z == L - 1 ? 0 : z + 1;
-    extern __shared__ __align__(128) uint4 sp[];  // own z | other z-1 | other z | other z+1
-    __shared__ __align__(8) uint64_t bar;
-    const uint32_t plane_bytes = (uint32_t)PL * 16;
-    if (threadIdx.x == 0) mbar_init(&bar, 1);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        mbar_expect_tx(&bar, 4 * plane_bytes);
-        bulk_load(sp, Sc + (size_t)z * PL, plane_bytes, &bar);
-        bulk_load(sp + PL, So + (size_t)zm * PL, plane_bytes, &bar);
-        bulk_load(sp + 2 * PL, So + (size_t)z * PL, plane_bytes, &bar);
-        bulk_load(sp + 3 * PL, So + (size_t)zp * PL, plane_bytes, &bar);
-    }
-    const uint32_t ctr3 = kTagSweep | ((uint32_t)c << 8) | (uint32_t)q;
-    const uint32_t wg = (uint32_t)w + P.word0;
-    uint32_t th0[4], th1[4], th2[4];
+        const uint32_t rr[4] = {r.v0, r.v1, r.v2, r.v3};
+        uint32_t cw[4] = {cv.x, cv.y, cv.z, cv.w};
+        const uint32_t n0w[4] = {a0.x, a0.y, a0.z, a0.w}, n1w[4] = {a1.x, a1.y, a1.z, a1.w};
+        const uint32_t n2w[4] = {a2.x, a2.y, a2.z, a2.w}, n3w[4] = {a3.x, a3.y, a3.z, a3.w};
+        const uint32_t n4w[4] = {a4.x, a4.y, a4.z, a4.w}, n5w[4] = {a5.x, a5.y, a5.z, a5.w};
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const int t = 4 * q + k;
-        th0[k] = P.tab.thr[t][0][0];
-        th1[k] = P.tab.thr[t][0][1];
-        th2[k] = P.tab.thr[t][0][2];
-    }
-    constexpr int NLV = kStreamNLV;
-    constexpr int NLM = kStreamNLM;
-    uint32_t ecnt[4][NLV], mcnt[4][NLM];
+        for (int k = 0; k < 4; ++k) {
+            const uint32_t s0 = cw[k];
+            const uint32_t u0 = s0 ^ n0w[k] ^ f0, u1 = s0 ^ n1w[k] ^ f1;
+            const uint32_t u2 = s0 ^ n2w[k] ^ f2, u3 = s0 ^ n3w[k] ^ f3;
+            const uint32_t u4 = s0 ^ n4w[k] ^ f4, u5 = s0 ^ n5w[k] ^ f5;
+            const uint32_t sa = u0 ^ u1 ^ u2, ca = maj3(u0, u1, u2);
+            const uint32_t sb = u3 ^ u4 ^ u5, cb = maj3(u3, u4, u5);
+            uint32_t fl;
+            if constexpr (GEN_H)
+                fl = flip_gen(s0, sa, ca, sb, cb, rr[k], &P.tab.thr[4 * q + k][0][0],
+                              &P.tab.ucut[4 * q + k][0]);
+            else
+                fl = flip_h0(sa, ca, sb, cb, rr[k], th0[k], th1[k], th2[k]);
+            cw[k] = s0 ^ fl;
+            // post-flip unsatisfied bonds (energy) and spins up, counted at once
+            if constexpr (ACC_E) vc_add_site<NLV>(ecnt[k], sa ^ fl, sb ^ fl, ca ^ fl, cb ^ fl);
+            if constexpr (ACC_M) {
+                uint32_t carry = cw[k];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-#pragma unroll
-        for (int l = 0; l < NLV; ++l) ecnt[k][l] = 0;
-#pragma unroll
-        for (int l = 0; l < NLM; ++l) mcnt[k][l] = 0;
-    }
-    bool ok = false;
-    for (int i = 0; i < kWaitTries && !ok; ++i) ok = mbar_try_wait(&bar, 0);
-    if (__syncthreads_or(!ok)) {  // the same decision in every thread
-        if (threadIdx.x == 0) atomicExch(P.err, 1);
-        // copies may still be landing in this block's shared memory
-        for (int i = 0; i < kWaitTries && !mbar_try_wait(&bar, 0); ++i) {
+                for (int l = 0; l < NLM; ++l) {
+                    const uint32_t t = mcnt[k][l] & carry;
+                    mcnt[k][l] ^= carry;
+                    carry = t;
+                }
+            }
         }
-        return;
-    }
-    const uint4* own = sp;
-    const uint4* om = sp + PL;
-    const uint4* oc = sp + 2 * PL;
-    const uint4* op = sp + 3 * PL;
-    const int zb = z * PL;
+        Sc[n] = make_uint4(cw[0], cw[1], cw[2], cw[3]);
+    };
+    // one site at a time: two per iteration (more registers, fewer resident
+    // blocks) measured slower at L=48
 #pragma unroll 1
-    for (int i = threadIdx.x; i < PL; i += kStreamThreads) {
-        const int y = div_magic(i, LH, P.mag_row);
-        const int h = i - y * LH;
-        const int o = (y + z + p) & 1;
-        const int x = 2 * h + o;
-        const int nxm = o ? i : (h == 0 ? i + LH - 1 : i - 1);
-        const int nxp = o ? (h == LH - 1 ? i - h : i + 1) : i;
-        const int nym = y == 0 ? i + PL - LH : i - LH;
-        const int nyp = y == L - 1 ? i - PL + LH : i + LH;
-        const uint4 a[6] = {oc[nxm], oc[nxp], oc[nym], oc[nyp], om[i], op[i]};
-        const int n = zb + i;
-        const uint32_t f[6] = {__ldg(Fo + zb + nxm), __ldg(Fc + n), __ldg(Fo + N + zb + nym),
-                               __ldg(Fc + N + n), __ldg(Fo + 2 * N + zm * PL + i),
-                               __ldg(Fc + 2 * N + n)};
-        const u32x4 r = philox4x32_10((uint32_t)((z * L + y) * L + x), (uint32_t)s, wg, ctr3,
-                                      P.k0, P.k1);
-        Sc[n] = stream_site_update<GEN_H, ACC_E, ACC_M, NLV, NLM>(P, q, own[i], a, f, r, th0, th1,
-                                                                  th2, ecnt, mcnt);
+    for (int m = 0; m < kStreamSPT; ++m) update_site(n_base + m * BT);
+    __shared__ int sred[2][4][32];
+    if (ACC_E || ACC_M) {
+        for (int i = threadIdx.x; i < 2 * 4 * 32; i += BT) (&sred[0][0][0])[i] = 0;
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if constexpr (ACC_E) atomicAdd(&sred[0][k][lane], column_count<NLV>(ecnt[k], lane));
+            if constexpr (ACC_M) atomicAdd(&sred[1][k][lane], column_count<NLM>(mcnt[k], lane));
+        }
+        __syncthreads();
+        if (threadIdx.x < 128) {
+            const int k = threadIdx.x >> 5;
+            if constexpr (ACC_E)
+                P.e_part[(((size_t)gq * P.nblk + blockIdx.y) * 4 + k) * 32 + lane] = sred[0][k][lane];
+            if constexpr (ACC_M)
+                P.m_part[((((size_t)gq * 2 + p) * P.nblk + blockIdx.y) * 4 + k) * 32 + lane] =
+                    sred[1][k][lane];
+        }
     }
-    stream_store_partials<ACC_E, ACC_M, NLV, NLM>(P, gq, p, ecnt, mcnt);
 }
 
 // Exchange decisions of one round: block = (w, c), one warp per pair.  Also
