@@ -217,6 +217,18 @@ int csg_set_plan_override(const csg_plan* plan);
 int csg_obs_records_noalloc(const csg_config* cfg, const uint32_t* spins, const uint32_t* bonds,
                             float* rec, size_t n_floats, void* stream);
 
+/* analyze-all.py:38-71 (the reference's analysis script): the result table of
+ * a record series on the GPU.  rec: device pointer to n_meas * ndis * nrep
+ * records (obs_s, 11 floats, the layout of <H>-obs.bin) - pass the part after
+ * the thermalisation, as the script drops the first half.  table: host array
+ * [nrep][8] receiving chi_0, its error, xi_L/L, its error, e, its error, m, its
+ * error (the script's estimators; the error is the standard error over
+ * disorder samples).  Runs on stream (NULL: the default stream) and returns
+ * when the table is ready; takes ndis * nrep * 72 bytes of stream-ordered
+ * scratch. */
+int csg_analyze_records(const float* rec, int64_t n_meas, int32_t ndis, int32_t nrep, int32_t L,
+                        double* table, void* stream);
+
 /* ---- Batched engine -------------------------------------------------------
  * No counterpart in the reference, which compiles one lattice size into its
  * binary (eamsim.cuh:13) and runs one simulation per process.  A batch holds

@@ -112,6 +112,7 @@ def lib():
             "csg_server_poll": [vp, vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                 C.POINTER(C.c_int32)],
             "csg_server_result": [vp, i64, C.POINTER(ObservablesC), vp, sz],
+            "csg_analyze_records": [vp, i64, C.c_int32, C.c_int32, C.c_int32, vp, vp],
         }
         for name, args in sig.items():
             f = getattr(L, name)

@@ -62,6 +62,36 @@ def analyze(path: str, L: int, ndis: int, nrep: int, betas=None, chunk: int = 8)
             "m_err": np.sqrt(m.var(axis=0) / ndis), "n_meas": n}
 
 
+def analyze_gpu(path: str, L: int, ndis: int, nrep: int, betas=None, device: int = 0) -> dict:
+    """analyze() on the GPU (csg_analyze_records): the records after the
+    thermalisation half are copied to the device once and reduced there."""
+    import ctypes as C
+
+    import torch
+
+    try:
+        from . import lib, _check
+    except ImportError:  # loaded as a plain module next to the package's __init__
+        pkg = sys.modules["spin_glass_b200"]
+        lib, _check = pkg.lib, pkg._check
+    size = np.memmap(path, dtype=np.uint8, mode="r").size
+    data = np.memmap(path, dtype=OBS_DT, mode="r", offset=size // 2)
+    n = data.size // (ndis * nrep)
+    if n == 0:
+        raise ValueError("no records after the thermalisation half")
+    host = np.array(data[: n * ndis * nrep]).view(np.float32)  # a writable copy
+    dev = torch.from_numpy(host).to(torch.device("cuda", device))
+    table = np.zeros((nrep, 8), np.float64)
+    _check(lib().csg_analyze_records(C.c_void_p(dev.data_ptr()), n, ndis, nrep, L,
+                                     table.ctypes.data_as(C.c_void_p), None))
+    if betas is None:
+        betas = np.logspace(1, -3, num=nrep, base=2.0)
+    cols = ["chi0", "chi0_err", "xi", "xi_err", "e", "e_err", "m", "m_err"]
+    res = {"beta": np.asarray(betas), "n_meas": n}
+    res.update({c: table[:, k] for k, c in enumerate(cols)})
+    return res
+
+
 def write_table(res: dict, path: str, sweeps_per_meas: int = 1024) -> None:
     with open(path, "w") as f:
         f.write(f"# tot_MC_steps : {2 * res['n_meas'] * sweeps_per_meas:,}\n")
