@@ -56,6 +56,9 @@ CASES = [
     (12, 1, 2, 8, 1.7, 16, 2, 1, 0),
     (18, 1, 2, 4, 0.0, 6, 1, 1, 0),
     (24, 1, 2, 8, 0.0, 4, 1, 1, 0),
+    (8, 1, 2, 64, 0.0, 8, 1, 1, 0),    # the largest ladder
+    (6, 3, 1, 4, 0.2, 10, 2, 3, 1),    # the smallest ladder, one copy, H != 0
+    (20, 1, 2, 12, 0.0, 5, 1, 1, 2),
 ]
 
 

@@ -54,6 +54,8 @@ STREAM_CASES = [
     (8, 2, 2, 12, 0.0, 20, 1, 1, 0, True),
     (12, 1, 2, 8, 1.3, 16, 2, 1, 3, True),
     (16, 1, 1, 24, 0.0, 10, 3, 2, 0, True),
+    (26, 1, 2, 64, 0.0, 3, 1, 1, 0, False),   # the largest ladder
+    (34, 1, 2, 4, 1.1, 3, 1, 1, 0, False),
 ]
 
 
