@@ -291,11 +291,12 @@ struct StreamLayout {
 StreamLayout stream_layout(const csg_config& c) {
     const csg_dims& d = c.dims;
     const size_t N = (size_t)d.L * d.L * d.L, Q = (size_t)d.n_temps / 4;
-    const size_t spb = csg::kStreamSitesPerBlock, spa = csg::kStreamAccSitesPerBlock;
+    const size_t spb = (size_t)csg::kStreamThreads * csg::kStreamSPT;
+    const size_t spa = csg::kStreamAccSitesPerBlock, spo = csg::kOverlapSitesPerBlock;
     StreamLayout s;
     s.nblk = (int)((N / 2 + spa - 1) / spa);  // blocks of the counting colour launches
     s.nblk_plain = (int)((N / 2 + spb - 1) / spb);
-    s.nblk2 = (int)((N + spb - 1) / spb);
+    s.nblk2 = (int)((N + spo - 1) / spo);
     const size_t quads = (size_t)d.n_words * d.n_copies * Q;
     const size_t planes = (size_t)d.n_words * d.n_copies * d.n_temps;
     auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };

@@ -18,18 +18,27 @@
 
 namespace csg {
 
+// Launch shapes (measured at L=32 and L=48).  Plain colour launches: blocks of
+// kStreamThreads threads, kStreamSPT sites of the colour per thread.
 constexpr int kStreamThreads = 256;
-constexpr int kStreamSPT = 8;  // sites of one colour per thread per launch
-constexpr int kStreamSitesPerBlock = kStreamThreads * kStreamSPT;
-// Colour launches that count (energies, magnetisations) hold ~40 more
-// registers per thread; they run blocks of half the size so that more blocks
-// stay resident.  Their partial sums are per block of this many sites.
+constexpr int kStreamSPT = 8;
+// Colour launches that count (energies, magnetisations) hold more registers
+// (the bit-sliced counters grow with the sites per thread); their partial sums
+// are per block of kStreamAccSitesPerBlock sites.
 constexpr int kStreamAccThreads = 128;
-constexpr int kStreamAccSitesPerBlock = kStreamAccThreads * kStreamSPT;
+constexpr int kStreamAccSPT = 8;
+constexpr int kStreamAccSitesPerBlock = kStreamAccThreads * kStreamAccSPT;
 template <bool ACC>
 __host__ __device__ constexpr int colour_threads() { return ACC ? kStreamAccThreads : kStreamThreads; }
-constexpr int kStreamNLV = bit_length(6 * kStreamSPT);  // bits of a per-thread bond count
-constexpr int kStreamNLM = bit_length(kStreamSPT);      // bits of a per-thread site count
+template <bool ACC>
+__host__ __device__ constexpr int colour_spt() { return ACC ? kStreamAccSPT : kStreamSPT; }
+constexpr int kStreamNLV = bit_length(6 * kStreamAccSPT);  // bits of a per-thread bond count
+constexpr int kStreamNLM = bit_length(kStreamAccSPT);      // bits of a per-thread site count
+// Overlap passes (both copies of every quad): blocks of kStreamThreads threads
+// over kOverlapSitesPerBlock sites (all N sites of a lattice).
+constexpr int kOverlapSPT = 8;
+constexpr int kOverlapSitesPerBlock = kStreamThreads * kOverlapSPT;
+constexpr int kOverlapNL = bit_length(kOverlapSPT);
 
 struct StreamParams {
     uint32_t* spins;
@@ -72,8 +81,8 @@ struct StreamObs {
 };
 
 // One colour of one sweep.  blockIdx.x = quad (w, c, q), blockIdx.y = block
-// of kStreamSPT * blockDim.x sites of that colour; each thread updates
-// kStreamSPT sites in the 4 planes of the quad.  Consecutive blocks take the
+// of colour_spt * blockDim.x sites of that colour; each thread updates
+// colour_spt sites in the 4 planes of the quad.  Consecutive blocks take the
 // quads of one word at the same sites, so the word's bonds are read once from
 // DRAM and then from L2.
 template <bool GEN_H, bool ACC_E, bool ACC_M>
@@ -112,8 +121,8 @@ __global__ void __launch_bounds__(colour_threads<ACC_E || ACC_M>()) stream_colou
         for (int l = 0; l < NLM; ++l) mcnt[k][l] = 0;
     }
     const int PL = L * LH;  // sites of one colour in one z plane
-    constexpr int BT = colour_threads<ACC_E || ACC_M>();
-    const int n_base = blockIdx.y * (BT * kStreamSPT) + threadIdx.x;
+    constexpr int BT = colour_threads<ACC_E || ACC_M>(), SPT = colour_spt<ACC_E || ACC_M>();
+    const int n_base = blockIdx.y * (BT * SPT) + threadIdx.x;
     auto update_site = [&](const int n) {
         if (n >= (int)NH) return;
         // n = (z L + y) L/2 + h; divisions by multiply-high
@@ -174,7 +183,7 @@ __global__ void __launch_bounds__(colour_threads<ACC_E || ACC_M>()) stream_colou
     // one site at a time: two per iteration (more registers, fewer resident
     // blocks) measured slower at L=48
 #pragma unroll 1
-    for (int m = 0; m < kStreamSPT; ++m) update_site(n_base + m * BT);
+    for (int m = 0; m < SPT; ++m) update_site(n_base + m * BT);
     __shared__ int sred[2][4][32];
     if (ACC_E || ACC_M) {
         for (int i = threadIdx.x; i < 2 * 4 * 32; i += BT) (&sred[0][0][0])[i] = 0;
@@ -307,7 +316,9 @@ __global__ void stream_exchange_kernel(const __grid_constant__ StreamParams P, i
 // d_part in the layout of stream_overlap_kernel.
 __global__ void __launch_bounds__(kStreamThreads) stream_exchange_overlap_kernel(
     const __grid_constant__ StreamParams P, int par) {
-    constexpr int kSites = 4, kGroups = kStreamSitesPerBlock / (kStreamThreads * kSites);
+    constexpr int kSites = 4, kGroups = kOverlapSitesPerBlock / (kStreamThreads * kSites);
+    static_assert(kGroups >= 1 && kGroups * kStreamThreads * kSites == kOverlapSitesPerBlock,
+                  "a block covers whole groups of 4 sites per thread");
     const int N = P.L * P.L * P.L, T = P.T, Q = P.Q;
     const int w = blockIdx.x, blk = blockIdx.y, lane = threadIdx.x & 31;
     __shared__ int sD[kMaxT][32];
@@ -321,7 +332,7 @@ __global__ void __launch_bounds__(kStreamThreads) stream_exchange_overlap_kernel
         int site[kSites];
 #pragma unroll
         for (int i = 0; i < kSites; ++i)
-            site[i] = blk * kStreamSitesPerBlock + (grp * kSites + i) * kStreamThreads + threadIdx.x;
+            site[i] = blk * kOverlapSitesPerBlock + (grp * kSites + i) * kStreamThreads + threadIdx.x;
         uint4 prv[2][kSites], cur[2][kSites];
         // store quad qq and add its overlap counts
         auto finish = [&](int qq, uint4 (&v)[2][kSites]) {
@@ -385,21 +396,21 @@ __global__ void __launch_bounds__(kStreamThreads) stream_exchange_overlap_kernel
 }
 
 // Overlap partial sums: blockIdx.x = (w, q), blockIdx.y = block of sites;
-// each thread kStreamSPT sites.
+// each thread kOverlapSPT sites.
 __global__ void __launch_bounds__(kStreamThreads) stream_overlap_kernel(const __grid_constant__ StreamParams P) {
     const long N = (long)P.L * P.L * P.L;
     const int wq = blockIdx.x, w = wq / P.Q, q = wq % P.Q;
     const int lane = threadIdx.x & 31;
     const uint4* A = reinterpret_cast<const uint4*>(P.spins) + ((size_t)(w * P.C + 0) * P.Q + q) * N;
     const uint4* B = reinterpret_cast<const uint4*>(P.spins) + ((size_t)(w * P.C + 1) * P.Q + q) * N;
-    constexpr int NL = kStreamNLM;
+    constexpr int NL = kOverlapNL;
     uint32_t dc[4][NL];
 #pragma unroll
     for (int k = 0; k < 4; ++k)
 #pragma unroll
         for (int l = 0; l < NL; ++l) dc[k][l] = 0;
-    const long n_base = (long)blockIdx.y * kStreamSitesPerBlock + threadIdx.x;
-    for (int m = 0; m < kStreamSPT; ++m) {
+    const long n_base = (long)blockIdx.y * kOverlapSitesPerBlock + threadIdx.x;
+    for (int m = 0; m < kOverlapSPT; ++m) {
         const long n = n_base + (long)m * kStreamThreads;
         uint4 x = make_uint4(0, 0, 0, 0);
         if (n < N) {
