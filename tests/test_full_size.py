@@ -28,6 +28,8 @@ SHAPES = [
     # L, words, temperatures, T range, sweeps
     (16, 32, 24, (0.2, 2.0), 12),   # production (cluster-resident kernel)
     (48, 8, 32, (0.5, 2.0), 6),     # large lattice (streaming engine)
+    (128, 1, 4, (0.5, 2.0), 2),     # the largest lattice side
+    (8, 64, 16, (0.5, 2.0), 6),     # many sample words (2048 samples) at small L
 ]
 
 
