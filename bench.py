@@ -62,13 +62,13 @@ def engine_flags(csg, args) -> int:
 
 
 def workload_config(n_gpus: int, swap_every: int = 1, measure_every: int = 1,
-                    engine: str = "auto") -> dict:
+                    engine: str = "auto", field: float = 0.0) -> dict:
     name = "plain PT engine, production size" + (" (streaming engine)" if engine == "stream" else "")
     return {"workload": name, "L": L, "samples": 32 * W,
             "copies": NCOPY, "temperatures": T, "T_range": [T_MIN, T_MAX],
             "sweeps_per_step": SWEEPS_PER_STEP, "swap_every": swap_every,
             "measure_every": measure_every,
-            "field_H": 0.0, "l2": "flushed between timed steps (256 MiB write)",
+            "field_H": field, "l2": "flushed between timed steps (256 MiB write)",
             "parallelism": f"sample shards x{n_gpus}"}
 
 
@@ -251,7 +251,8 @@ def run_ours(args, rank: int, world: int, dist) -> None:
     dev = torch.device("cuda", local)
     seed = SEED  # one simulation of world x 1024 samples, sharded by sample word
     betas = 1.0 / (T_MIN * (T_MAX / T_MIN) ** (np.arange(T) / (T - 1)))
-    cfg, _keep = csg.make_config(L, W, NCOPY, betas, seed=seed, sweeps_per_swap=args.swap_every,
+    cfg, _keep = csg.make_config(L, W, NCOPY, betas, H=args.field, seed=seed,
+                                 sweeps_per_swap=args.swap_every,
                                  sweeps_per_meas=args.measure_every, meas_start=0, word0=rank * W,
                                  flags=engine_flags(csg, args))
     N = L ** 3
@@ -317,7 +318,8 @@ def run_ours(args, rank: int, world: int, dist) -> None:
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic (seeded +-J disorder, uniform random initial spins)",
-            "config": workload_config(world, args.swap_every, args.measure_every, args.engine),
+            "config": workload_config(world, args.swap_every, args.measure_every, args.engine,
+                                      args.field),
             "roofline": {"bound": "int", "achieved": achieved / 1e12, "peak": peak["ops_per_s"] / 1e12,
                          "unit": "Tops/s (32-bit integer logic)",
                          "frac": achieved / peak["ops_per_s"], "traffic": profile_traffic(),
@@ -340,7 +342,7 @@ def run_e2e(csg, torch, betas, seed, args, word0: int = 0) -> dict:
     N = L ** 3
     hs = torch.empty(W * NCOPY * T * N, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
     hb = torch.empty(W * 3 * N, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
-    with csg.Engine(L, W, NCOPY, betas, seed=seed, sweeps_per_swap=args.swap_every,
+    with csg.Engine(L, W, NCOPY, betas, H=args.field, seed=seed, sweeps_per_swap=args.swap_every,
                     sweeps_per_meas=args.measure_every, word0=word0,
                     flags=engine_flags(csg, args)) as eng:
         eng.init_lattice()
@@ -689,6 +691,8 @@ def main() -> None:
                     help="sweeps per measurement (0: none; default 1, mixed: 1024)")
     ap.add_argument("--workload", choices=["production", "mixed", "serving", "large"],
                     default="production")
+    ap.add_argument("--field", type=float, default=0.0,
+                    help="production workload: external field H (H != 0: general-field kernel)")
     ap.add_argument("--engine", choices=["auto", "stream"], default="auto",
                     help="production workload: stream = force the streaming engine")
     ap.add_argument("--serve-rate", type=float, default=2.0, help="requests per second")

@@ -101,6 +101,8 @@ bool build_tables(const csg_config& cfg, csg::PtTables& tab) {
             }
             tab.ucut[t][s] = (uint8_t)cut;
             if (cut != 3) h0_exact = false;
+            // cut <= 3 (s = 0) and cut <= 5 (s = 1) for 0 <= H <= 4 (validate()),
+            // as the general-field rule (flip_gen) requires
         }
         for (int U = 0; U < 3; ++U)
             if (tab.thr[t][0][U] != tab.thr[t][1][U]) h0_exact = false;

@@ -221,26 +221,44 @@ __device__ __forceinline__ uint32_t flip_h0(uint32_t sa, uint32_t ca, uint32_t s
     return f;
 }
 
-// General field: thresholds depend on the centre spin; for each spin value
-// the accepted set is {U >= m(r)}.
+// General field, 0 <= H <= 4.  A flip of centre spin s with U unsatisfied
+// bonds is accepted iff U >= ucut_s (dE <= 0) or the draw r < thr[s][U].
+// thr[s][U] does not decrease with U and is 0xFFFFFFFF from ucut_s on, and
+// ucut_0 <= 3, ucut_1 <= 5, so walking U down from there the accepted set is
+// {U >= the smallest U with r < thr[s][U]} - a select chain like the H = 0
+// rule.  Only the draw r = 0xFFFFFFFF, below none of the thresholds, needs the
+// cut itself.  ta = {thr0[0], thr0[1], thr0[2], thr1[0]},
+// tb = {thr1[1], thr1[2], thr1[3], thr1[4]}.
 __device__ __forceinline__ uint32_t flip_gen(uint32_t s0, uint32_t sa, uint32_t ca, uint32_t sb,
-                                             uint32_t cb, uint32_t r, const uint32_t* thr,
-                                             const uint8_t* ucut) {
+                                             uint32_t cb, uint32_t r, const uint4 ta, const uint4 tb,
+                                             int uc0, int uc1) {
     // U = sa + sb + 2(ca + cb): U >= 4 needs both carries, or one carry and
     // both sum bits; U >= 5 and U >= 6 need both carries.
-    const uint32_t v = sa | sb;
-    const uint32_t cc = ca & cb;
-    const uint32_t ge[7] = {0xFFFFFFFFu, ca | cb | v, ca | cb | (sa & sb), maj3(ca, cb, v),
-                            cc | ((ca | cb) & sa & sb), cc & v, cc & sa & sb};
-    uint32_t g0 = 0, g1 = 0;
-#pragma unroll
-    for (int U = 6; U >= 0; --U) {
-        const bool a0 = (U >= (int)ucut[0]) || (r < thr[U]);
-        const bool a1 = (U >= (int)ucut[1]) || (r < thr[7 + U]);
-        g0 = a0 ? ge[U] : g0;
-        g1 = a1 ? ge[U] : g1;
+    const uint32_t v = sa | sb, cx = ca | cb, cc = ca & cb;
+    const uint32_t ge1 = cx | v, ge2 = cx | (sa & sb), ge3 = maj3(ca, cb, v);
+    const uint32_t ge4 = cc | (cx & sa & sb), ge5 = cc & v;
+    uint32_t g0 = ge3;
+    g0 = (r < ta.z) ? ge2 : g0;
+    g0 = (r < ta.y) ? ge1 : g0;
+    g0 = (r < ta.x) ? 0xFFFFFFFFu : g0;
+    uint32_t g1 = ge5;
+    g1 = (r < tb.w) ? ge4 : g1;
+    g1 = (r < tb.z) ? ge3 : g1;
+    g1 = (r < tb.y) ? ge2 : g1;
+    g1 = (r < tb.x) ? ge1 : g1;
+    g1 = (r < ta.w) ? 0xFFFFFFFFu : g1;
+    if (r == 0xFFFFFFFFu) {  // accepted: exactly U >= ucut
+        const uint32_t ge[8] = {0xFFFFFFFFu, ge1, ge2, ge3, ge4, ge5, cc & sa & sb, 0u};
+        g0 = ge[uc0 & 7];
+        g1 = ge[uc1 & 7];
     }
     return (s0 & g1) | (~s0 & g0);
+}
+
+// The thresholds of plane t in the layout flip_gen takes.
+__host__ __device__ inline void gen_thresholds(const PtTables& tab, int t, uint4& ta, uint4& tb) {
+    ta = make_uint4(tab.thr[t][0][0], tab.thr[t][0][1], tab.thr[t][0][2], tab.thr[t][1][0]);
+    tb = make_uint4(tab.thr[t][1][1], tab.thr[t][1][2], tab.thr[t][1][3], tab.thr[t][1][4]);
 }
 
 // Shared-memory layout of one CTA (dynamic):
@@ -248,7 +266,7 @@ __device__ __forceinline__ uint32_t flip_gen(uint32_t s0, uint32_t sa, uint32_t 
 //   arrays, so that every access of one plane by a warp is conflict-free);
 //   int sE[Qc*4][32]; int sD[Qc*4][32];
 //   int sM[Qc*4][32]                      (only with magnetisations)
-//   uint32 sThr[Qc*4][2][7]; uint8 sUcut[Qc*4][2]   (only for H != 0)
+//   uint4 sThr[Qc*4][2]; uint8 sUcut[Qc*4][2]   (only for H != 0)
 // The exchange masks of a round live in the first 2*Qc words of sD, which is
 // cleared again before the overlap counts are added.  At L=16 with 3 quads the
 // H=0 layout is 195 KB, under the 196 KB carve-out, so the 48 KB of bonds of
@@ -257,7 +275,7 @@ template <int L>
 struct SmemMap {
     static __host__ __device__ size_t bytes(int Qc, bool has_m, bool gen) {
         return (size_t)Qc * LCfg<L>::N * 16 + (size_t)Qc * 4 * 32 * 4 * (has_m ? 3 : 2) +
-               (gen ? (size_t)Qc * 4 * 14 * 4 + (size_t)Qc * 4 * 2 : 0);
+               (gen ? (size_t)Qc * 4 * 32 + (size_t)Qc * 4 * 2 : 0);
     }
 };
 
@@ -300,8 +318,8 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
     int* sD = sE + Qc * 4 * 32;
     int* sM = sD + Qc * 4 * 32;  // valid only when has_M
     uint32_t* sMask = reinterpret_cast<uint32_t*>(sD);
-    uint32_t* sThr = reinterpret_cast<uint32_t*>(sM + (has_M ? Qc * 4 * 32 : 0));
-    uint8_t* sUcut = reinterpret_cast<uint8_t*>(sThr + Qc * 4 * 14);
+    uint4* sThr = reinterpret_cast<uint4*>(sM + (has_M ? Qc * 4 * 32 : 0));  // 16-byte aligned
+    uint8_t* sUcut = reinterpret_cast<uint8_t*>(sThr + Qc * 4 * 2);
 
     // global offset of local quad jj (layout [W][C][T/4][N])
     auto quad_base = [&](int jj) {
@@ -317,11 +335,10 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
         }
     }
     if constexpr (GEN_H) {
-        for (int i = tid; i < Qc * 4 * 14; i += nthreads) {
-            const int pl = i / 14, k = i - pl * 14;
+        for (int pl = tid; pl < Qc * 4; pl += nthreads) {
             const int gg = rank * Qc + pl / 4;
             const int t = 4 * (gg / C) + (pl & 3);
-            sThr[i] = P.tab.thr[t][k / 7][k % 7];
+            gen_thresholds(P.tab, t, sThr[2 * pl], sThr[2 * pl + 1]);
         }
         for (int i = tid; i < Qc * 4 * 2; i += nthreads) {
             const int pl = i / 2;
@@ -344,7 +361,7 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
     const uint32_t* Fw = P.bonds + (size_t)w * 3 * N;
     const uint32_t ctr3 = kTagSweep | ((uint32_t)c << 8) | (uint32_t)q;
     const uint32_t wg = (uint32_t)w + P.word0;  // global sample word
-    const uint32_t* thrq = sThr + (size_t)j * 4 * 14;
+    const uint4* thrq = sThr + (size_t)j * 4 * 2;
     const uint8_t* ucq = sUcut + (size_t)j * 4 * 2;
 
     const long long sweep_base = P.sweep0 + (P.sweep_dev ? *P.sweep_dev : 0ll);
@@ -420,7 +437,8 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
                             const uint32_t sb = u3 ^ u4 ^ u5, cb = maj3(u3, u4, u5);
                             uint32_t fl;
                             if constexpr (GEN_H)
-                                fl = flip_gen(s0, sa, ca, sb, cb, rr[k], thrq + k * 14, ucq + k * 2);
+                                fl = flip_gen(s0, sa, ca, sb, cb, rr[k], thrq[2 * k], thrq[2 * k + 1],
+                                              ucq[2 * k], ucq[2 * k + 1]);
                             else
                                 fl = flip_h0(sa, ca, sb, cb, rr[k], th0[k], th1[k], th2[k]);
                             cw[k] = s0 ^ fl;

@@ -160,11 +160,14 @@ __global__ void __launch_bounds__(colour_threads<ACC_E || ACC_M>()) stream_colou
             const uint32_t sa = u0 ^ u1 ^ u2, ca = maj3(u0, u1, u2);
             const uint32_t sb = u3 ^ u4 ^ u5, cb = maj3(u3, u4, u5);
             uint32_t fl;
-            if constexpr (GEN_H)
-                fl = flip_gen(s0, sa, ca, sb, cb, rr[k], &P.tab.thr[4 * q + k][0][0],
-                              &P.tab.ucut[4 * q + k][0]);
-            else
-                fl = flip_h0(sa, ca, sb, cb, rr[k], th0[k], th1[k], th2[k]);
+        if constexpr (GEN_H) {
+            uint4 ta, tb;
+            gen_thresholds(P.tab, 4 * q + k, ta, tb);
+            fl = flip_gen(s0, sa, ca, sb, cb, rr[k], ta, tb, P.tab.ucut[4 * q + k][0],
+                          P.tab.ucut[4 * q + k][1]);
+        } else {
+            fl = flip_h0(sa, ca, sb, cb, rr[k], th0[k], th1[k], th2[k]);
+        }
             cw[k] = s0 ^ fl;
             // post-flip unsatisfied bonds (energy) and spins up, counted at once
             if constexpr (ACC_E) vc_add_site<NLV>(ecnt[k], sa ^ fl, sb ^ fl, ca ^ fl, cb ^ fl);
