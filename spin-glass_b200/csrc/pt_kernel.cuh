@@ -362,7 +362,16 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
     const uint32_t ctr3 = kTagSweep | ((uint32_t)c << 8) | (uint32_t)q;
     const uint32_t wg = (uint32_t)w + P.word0;  // global sample word
     const uint4* thrq = sThr + (size_t)j * 4 * 2;
-    const uint8_t* ucq = sUcut + (size_t)j * 4 * 2;
+    // the cuts of this quad's 4 planes, one byte each (used only for r = 0xFFFFFFFF)
+    uint32_t uc0 = 0, uc1 = 0;
+    if constexpr (GEN_H) {
+        const uint8_t* ucq = sUcut + (size_t)j * 4 * 2;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            uc0 |= (uint32_t)ucq[2 * k] << (8 * k);
+            uc1 |= (uint32_t)ucq[2 * k + 1] << (8 * k);
+        }
+    }
 
     const long long sweep_base = P.sweep0 + (P.sweep_dev ? *P.sweep_dev : 0ll);
     for (int it = 0; it < P.n_sweeps; ++it) {
@@ -438,7 +447,8 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
                             uint32_t fl;
                             if constexpr (GEN_H)
                                 fl = flip_gen(s0, sa, ca, sb, cb, rr[k], thrq[2 * k], thrq[2 * k + 1],
-                                              ucq[2 * k], ucq[2 * k + 1]);
+                                              (int)((uc0 >> (8 * k)) & 0xFF),
+                                              (int)((uc1 >> (8 * k)) & 0xFF));
                             else
                                 fl = flip_h0(sa, ca, sb, cb, rr[k], th0[k], th1[k], th2[k]);
                             cw[k] = s0 ^ fl;
