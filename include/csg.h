@@ -184,7 +184,10 @@ int csg_load_checkpoint(csg_engine* e, const uint32_t* ref, size_t n_words, int6
 /* run_simulation_section (eamsim.cu:347-416) on caller-owned device buffers:
  * n_sweeps sweeps of `spins` (canonical layout, device memory) starting at
  * global sweep index sweep0, adding to the device accumulators of `obs`
- * (may be NULL).  stream: a cudaStream_t (NULL = legacy default stream). */
+ * (may be NULL).  stream: a cudaStream_t (NULL = legacy default stream).
+ * Queued on the stream; the cluster-resident kernel (L <= 24) allocates
+ * nothing, the streaming engine (L > 24 or CSG_ENGINE_STREAM) takes a few MB
+ * of stream-ordered scratch (cudaMallocAsync / cudaFreeAsync on the stream). */
 int csg_pt_run_device(const csg_config* cfg, uint32_t* spins, const uint32_t* bonds,
                       const csg_device_obs* obs, int64_t sweep0, int64_t n_sweeps, void* stream);
 
