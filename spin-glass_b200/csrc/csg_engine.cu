@@ -7,6 +7,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "csg.h"
@@ -313,6 +314,24 @@ StreamLayout stream_layout(const csg_config& c) {
     return s;
 }
 
+// A launch of the streaming engine's sweep sequence, with programmatic
+// dependent launch (the kernels wait for their predecessor in pdl_enter()).
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st,
+                       Args&&... args) {
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = grid;
+    lc.blockDim = block;
+    lc.dynamicSmemBytes = 0;
+    lc.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    lc.attrs = attr;
+    lc.numAttrs = 1;
+    return cudaLaunchKernelEx(&lc, kernel, std::forward<Args>(args)...);
+}
+
 using ColourLaunch = void (*)(const csg::StreamParams&, const StreamLayout&, int, long long,
                               cudaStream_t);
 
@@ -320,7 +339,7 @@ template <bool G, bool E, bool M>
 void launch_colour(const csg::StreamParams& S, const StreamLayout& lay, int p, long long s,
                    cudaStream_t st) {
     const dim3 grid((unsigned)(S.W * S.C * S.Q), (unsigned)(E || M ? lay.nblk : lay.nblk_plain));
-    csg::stream_colour_kernel<G, E, M><<<grid, csg::colour_threads<E || M>(), 0, st>>>(S, p, s);
+    launch_pdl(csg::stream_colour_kernel<G, E, M>, grid, dim3(csg::colour_threads<E || M>()), st, S, p, s);
 }
 
 ColourLaunch colour_launch(bool gen, bool acc_e, bool acc_m) {
@@ -407,19 +426,20 @@ int run_stream(const csg_config& cfg, uint32_t* spins, const uint32_t* bonds,
         if (need_E) {
             const long long round = do_swap ? (s + 1) / sps - 1 : 0;
             const int par = (int)(round & 1);
-            csg::stream_decide_kernel<<<W * C, std::min(1024, 32 * d.n_temps), 0, st>>>(
-                S, s, par, need_M, do_swap, boundary,
-                                                              swap_acc, swap_log, round - round0,
-                                                              log_rounds);
+            launch_pdl(csg::stream_decide_kernel, dim3(W * C), dim3(std::min(1024, 32 * d.n_temps)), st,
+                       S, s, par, need_M, do_swap, boundary, swap_acc, swap_log, round - round0,
+                       log_rounds);
             const bool overlap = do_meas && obs && C == 2;
             if (do_swap && overlap)  // one pass: exchange, then count the overlaps
-                csg::stream_exchange_overlap_kernel<<<dim3(W, (unsigned)lay.nblk2), csg::kStreamThreads, 0,
-                                                      st>>>(S, par);
+                launch_pdl(csg::stream_exchange_overlap_kernel, dim3(W, (unsigned)lay.nblk2),
+                           dim3(csg::kStreamThreads), st, S, par);
             else if (do_swap)
-                csg::stream_exchange_kernel<<<g_exchange, 256, 0, st>>>(S, par);
+                launch_pdl(csg::stream_exchange_kernel, g_exchange, dim3(256), st, S, par);
             else if (overlap)
-                csg::stream_overlap_kernel<<<g_overlap, csg::kStreamThreads, 0, st>>>(S);
-            if (do_meas && obs) csg::stream_measure_kernel<<<W * (unsigned)d.n_temps, 64, 0, st>>>(S, need_M, O);
+                launch_pdl(csg::stream_overlap_kernel, g_overlap, dim3(csg::kStreamThreads), st, S);
+            if (do_meas && obs)
+                launch_pdl(csg::stream_measure_kernel, dim3(W * (unsigned)d.n_temps), dim3(64), st, S,
+                           need_M, O);
         }
         ce = cudaGetLastError();
     }

@@ -80,6 +80,15 @@ struct StreamObs {
     int* d_last;
 };
 
+// Programmatic dependent launch (the sweep's kernels are launched with it): a
+// kernel waits here until the previous kernel on the stream has finished and
+// its writes are visible, then lets the next kernel's blocks be scheduled as
+// soon as all of its own blocks run, so launch latency overlaps the tail.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // One colour of one sweep.  blockIdx.x = quad (w, c, q), blockIdx.y = block
 // of colour_spt * blockDim.x sites of that colour; each thread updates
 // colour_spt sites in the 4 planes of the quad.  Consecutive blocks take the
@@ -87,8 +96,8 @@ struct StreamObs {
 // DRAM and then from L2.
 template <bool GEN_H, bool ACC_E, bool ACC_M>
 __global__ void __launch_bounds__(colour_threads<ACC_E || ACC_M>()) stream_colour_kernel(
-    const __grid_constant__ StreamParams P,
-                                                                       int p, long long s) {
+    const __grid_constant__ StreamParams P, int p, long long s) {
+    pdl_enter();
     const int L = P.L, LH = L / 2;
     const int N = L * L * L, NH = N / 2;
     const int gq = blockIdx.x;
@@ -232,6 +241,7 @@ __global__ void stream_decide_kernel(const __grid_constant__ StreamParams P, lon
                                      bool need_M, bool do_swap, unsigned long long* boundary,
                                      unsigned long long* swap_acc, unsigned int* swap_log,
                                      long long log_row, long long log_rows) {
+    pdl_enter();
     const int wc = blockIdx.x, w = wc / P.C, c = wc % P.C;
     const int T = P.T, N = P.L * P.L * P.L;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
@@ -293,6 +303,7 @@ __global__ void stream_decide_kernel(const __grid_constant__ StreamParams P, lon
 // Masked exchange: a thread takes one site of one (w, c) and every quad of it,
 // so both words of every pair (also across quads) are its own.
 __global__ void stream_exchange_kernel(const __grid_constant__ StreamParams P, int par) {
+    pdl_enter();
     const long N = (long)P.L * P.L * P.L;
     const int wc = blockIdx.x;
     const long n = (long)blockIdx.y * blockDim.x + threadIdx.x;
@@ -336,6 +347,7 @@ __global__ void stream_exchange_kernel(const __grid_constant__ StreamParams P, i
 // d_part in the layout of stream_overlap_kernel.
 __global__ void __launch_bounds__(kStreamThreads) stream_exchange_overlap_kernel(
     const __grid_constant__ StreamParams P, int par) {
+    pdl_enter();
     constexpr int kSites = 4, kGroups = kOverlapSitesPerBlock / (kStreamThreads * kSites);
     static_assert(kGroups >= 1 && kGroups * kStreamThreads * kSites == kOverlapSitesPerBlock,
                   "a block covers whole groups of 4 sites per thread");
@@ -418,6 +430,7 @@ __global__ void __launch_bounds__(kStreamThreads) stream_exchange_overlap_kernel
 // Overlap partial sums: blockIdx.x = (w, q), blockIdx.y = block of sites;
 // each thread kOverlapSPT sites.
 __global__ void __launch_bounds__(kStreamThreads) stream_overlap_kernel(const __grid_constant__ StreamParams P) {
+    pdl_enter();
     const long N = (long)P.L * P.L * P.L;
     const int wq = blockIdx.x, w = wq / P.Q, q = wq % P.Q;
     const int lane = threadIdx.x & 31;
@@ -466,6 +479,7 @@ __global__ void __launch_bounds__(kStreamThreads) stream_overlap_kernel(const __
 // threads also total the overlap partials of the plane.
 __global__ void stream_measure_kernel(const __grid_constant__ StreamParams P, bool need_M,
                                       StreamObs O) {
+    pdl_enter();
     const int w = blockIdx.x / P.T, t = blockIdx.x % P.T, T = P.T, N = P.L * P.L * P.L;
     const int c = threadIdx.x >> 5, b = threadIdx.x & 31;
     if (c < P.C) {
