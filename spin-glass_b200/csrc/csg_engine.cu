@@ -288,25 +288,24 @@ constexpr int64_t kSweepsPerLaunch = 1024;
 // ---------------------------------------------------------------------------
 struct StreamLayout {
     int nblk = 0, nblk_plain = 0, nblk2 = 0;
-    size_t e_part = 0, m_part = 0, d_part = 0, energy = 0, magn = 0, masks = 0, bytes = 0;
+    size_t u_acc = 0, up_acc = 0, d_acc = 0, energy = 0, magn = 0, masks = 0, bytes = 0;
 };
 
 StreamLayout stream_layout(const csg_config& c) {
     const csg_dims& d = c.dims;
-    const size_t N = (size_t)d.L * d.L * d.L, Q = (size_t)d.n_temps / 4;
+    const size_t N = (size_t)d.L * d.L * d.L;
     const size_t spb = (size_t)csg::kStreamThreads * csg::kStreamSPT;
     const size_t spa = csg::kStreamAccSitesPerBlock, spo = csg::kOverlapSitesPerBlock;
     StreamLayout s;
     s.nblk = (int)((N / 2 + spa - 1) / spa);  // blocks of the counting colour launches
     s.nblk_plain = (int)((N / 2 + spb - 1) / spb);
     s.nblk2 = (int)((N + spo - 1) / spo);
-    const size_t quads = (size_t)d.n_words * d.n_copies * Q;
     const size_t planes = (size_t)d.n_words * d.n_copies * d.n_temps;
     auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
     size_t off = 0;
-    s.e_part = off, off += up(quads * s.nblk * 128 * 4);
-    s.m_part = off, off += up(quads * 2 * s.nblk * 128 * 4);
-    s.d_part = off, off += up((size_t)d.n_words * Q * s.nblk2 * 128 * 4);
+    s.u_acc = off, off += up(planes * 32 * 4);
+    s.up_acc = off, off += up(planes * 32 * 4);
+    s.d_acc = off, off += up((size_t)d.n_words * d.n_temps * 32 * 4);
     s.energy = off, off += up(planes * 32 * 4);
     s.magn = off, off += up(planes * 32 * 4);
     s.masks = off, off += up(planes * 4);
@@ -402,9 +401,11 @@ int run_stream(const csg_config& cfg, uint32_t* spins, const uint32_t* bonds,
     }
     char* base = nullptr;
     CSG_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&base), lay.bytes, st));
-    S.e_part = reinterpret_cast<int*>(base + lay.e_part);
-    S.m_part = reinterpret_cast<int*>(base + lay.m_part);
-    S.d_part = reinterpret_cast<int*>(base + lay.d_part);
+    S.u_acc = reinterpret_cast<int*>(base + lay.u_acc);
+    S.up_acc = reinterpret_cast<int*>(base + lay.up_acc);
+    S.d_acc = reinterpret_cast<int*>(base + lay.d_acc);
+    // the totals start at zero; each consumer clears what it read
+    CSG_CUDA(cudaMemsetAsync(base + lay.u_acc, 0, lay.energy - lay.u_acc, st));
     S.energy = reinterpret_cast<int*>(base + lay.energy);
     S.magn = reinterpret_cast<int*>(base + lay.magn);
     S.masks = reinterpret_cast<uint32_t*>(base + lay.masks);

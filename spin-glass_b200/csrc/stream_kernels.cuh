@@ -43,9 +43,11 @@ constexpr int kOverlapNL = bit_length(kOverlapSPT);
 struct StreamParams {
     uint32_t* spins;
     const uint32_t* bonds;
-    int* e_part;  // [W*C*Q][nblk][4][32] unsatisfied-bond partial sums
-    int* m_part;  // [W*C*Q][2 colours][nblk][4][32] spin-up partial sums
-    int* d_part;  // [W*Q][nblk2][4][32] differing-site partial sums
+    // per-plane totals, added to by the blocks (integer atomics: any order gives
+    // the same sums) and cleared by the kernel that consumes them
+    int* u_acc;   // [W][C][T][32] unsatisfied bonds after the sweep
+    int* up_acc;  // [W][C][T][32] spins up after the sweep
+    int* d_acc;   // [W][T][32] sites where the copies differ
     int* energy;  // [W][C][T][32] bond energies after the exchange
     int* magn;    // [W][C][T][32]
     uint32_t* masks;  // [W][C][T] accepted-sample masks of the current round
@@ -225,11 +227,9 @@ __global__ void __launch_bounds__(colour_threads<ACC_E || ACC_M>()) stream_colou
         __syncthreads();
         if (threadIdx.x < 128) {
             const int k = threadIdx.x >> 5;
-            if constexpr (ACC_E)
-                P.e_part[(((size_t)gq * P.nblk + blockIdx.y) * 4 + k) * 32 + lane] = sred[0][k][lane];
-            if constexpr (ACC_M)
-                P.m_part[((((size_t)gq * 2 + p) * P.nblk + blockIdx.y) * 4 + k) * 32 + lane] =
-                    sred[1][k][lane];
+            const size_t o = (((size_t)w * P.C + c) * P.T + 4 * q + k) * 32 + lane;
+            if constexpr (ACC_E) atomicAdd(&P.u_acc[o], sred[0][k][lane]);
+            if constexpr (ACC_M) atomicAdd(&P.up_acc[o], sred[1][k][lane]);
         }
     }
 }
@@ -247,17 +247,16 @@ __global__ void stream_decide_kernel(const __grid_constant__ StreamParams P, lon
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     int* E = P.energy + (size_t)wc * T * 32;
     int* M = P.magn + (size_t)wc * T * 32;
-    // totals: one thread per (plane, sample), the partials of its plane's quad
+    // totals of every plane of this (word, copy), cleared for the next sweep
+    int* ua = P.u_acc + (size_t)wc * T * 32;
+    int* pa = P.up_acc + (size_t)wc * T * 32;
     for (int i = threadIdx.x; i < T * 32; i += blockDim.x) {
-        const int t = i >> 5, b = i & 31, q = t >> 2, k = t & 3, gq = wc * P.Q + q;
-        const int* ep = P.e_part + ((size_t)gq * P.nblk * 4 + k) * 32 + b;
-        int u = 0, up = 0;
-#pragma unroll 4
-        for (int blk = 0; blk < P.nblk; ++blk) u += ep[(size_t)blk * 128];
+        const int u = ua[i];
+        ua[i] = 0;
+        int up = 0;
         if (need_M) {
-            const int* mp = P.m_part + ((size_t)gq * 2 * P.nblk * 4 + k) * 32 + b;
-#pragma unroll 4
-            for (int blk = 0; blk < 2 * P.nblk; ++blk) up += mp[(size_t)blk * 128];
+            up = pa[i];
+            pa[i] = 0;
         }
         E[i] = 2 * u - 3 * N;
         M[i] = need_M ? 2 * up - N : 0;
@@ -344,7 +343,7 @@ __global__ void stream_exchange_kernel(const __grid_constant__ StreamParams P, i
 // final only after its pair (3 of q, 0 of q+1) is exchanged, so each quad is
 // written (and its overlap counted) one step after it is loaded.  Every word
 // is read and written by exactly one thread.  Partial overlap counts go to
-// d_part in the layout of stream_overlap_kernel.
+// d_acc, like stream_overlap_kernel's.
 __global__ void __launch_bounds__(kStreamThreads) stream_exchange_overlap_kernel(
     const __grid_constant__ StreamParams P, int par) {
     pdl_enter();
@@ -423,7 +422,7 @@ __global__ void __launch_bounds__(kStreamThreads) stream_exchange_overlap_kernel
     __syncthreads();
     for (int i = threadIdx.x; i < T * 32; i += kStreamThreads) {
         const int t = i >> 5, b = i & 31;
-        P.d_part[((((size_t)w * Q + (t >> 2)) * P.nblk2 + blk) * 4 + (t & 3)) * 32 + b] = sD[t][b];
+        atomicAdd(&P.d_acc[((size_t)w * T + t) * 32 + b], sD[t][b]);
     }
 }
 
@@ -470,7 +469,7 @@ __global__ void __launch_bounds__(kStreamThreads) stream_overlap_kernel(const __
     __syncthreads();
     if (threadIdx.x < 128) {
         const int k = threadIdx.x >> 5;
-        P.d_part[(((size_t)wq * P.nblk2 + blockIdx.y) * 4 + k) * 32 + lane] = sred[k][lane];
+        atomicAdd(&P.d_acc[((size_t)w * P.T + 4 * q + k) * 32 + lane], sred[k][lane]);
     }
 }
 
@@ -493,11 +492,9 @@ __global__ void stream_measure_kernel(const __grid_constant__ StreamParams P, bo
         }
     }
     if (P.C != 2 || c != 0) return;
-    const int q = t >> 2, k = t & 3;
-    const int* dp = P.d_part + ((size_t)(w * P.Q + q) * P.nblk2 * 4 + k) * 32 + b;
-    int D = 0;
-#pragma unroll 4
-    for (int blk = 0; blk < P.nblk2; ++blk) D += dp[(size_t)blk * 128];
+    int* dp = P.d_acc + ((size_t)w * T + t) * 32 + b;
+    const int D = *dp;
+    *dp = 0;
     const long long Qv = (long long)N - 2LL * D;
     const unsigned long long q2 = (unsigned long long)(Qv * Qv);
     const size_t o = ((size_t)w * T + t) * 32 + b;
