@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(colour_threads<ACC_E || ACC_M>()) stream_colou
     const int PL = L * LH;  // sites of one colour in one z plane
     constexpr int BT = colour_threads<ACC_E || ACC_M>(), SPT = colour_spt<ACC_E || ACC_M>();
     const int n_base = blockIdx.y * (BT * SPT) + threadIdx.x;
-    auto update_site = [&](const int n) {
+    auto update_site = [&](const int n, uint32_t (&wd)[4][4]) {
         if (n >= (int)NH) return;
         // n = (z L + y) L/2 + h; divisions by multiply-high
         const int z = div_magic(n, PL, P.mag_plane);
@@ -173,23 +173,21 @@ __global__ void __launch_bounds__(colour_threads<ACC_E || ACC_M>()) stream_colou
             const uint32_t sa = u0 ^ u1 ^ u2, ca = maj3(u0, u1, u2);
             const uint32_t sb = u3 ^ u4 ^ u5, cb = maj3(u3, u4, u5);
             uint32_t fl;
-        if constexpr (GEN_H) {
-            uint4 ta, tb;
-            gen_thresholds(P.tab, 4 * q + k, ta, tb);
-            fl = flip_gen(s0, sa, ca, sb, cb, rr[k], ta, tb, P.tab.ucut[4 * q + k][0],
-                          P.tab.ucut[4 * q + k][1]);
-        } else {
-            fl = flip_h0(sa, ca, sb, cb, rr[k], th0[k], th1[k], th2[k]);
-        }
+            if constexpr (GEN_H) {
+                uint4 ta, tb;
+                gen_thresholds(P.tab, 4 * q + k, ta, tb);
+                fl = flip_gen(s0, sa, ca, sb, cb, rr[k], ta, tb, P.tab.ucut[4 * q + k][0],
+                              P.tab.ucut[4 * q + k][1]);
+            } else {
+                fl = flip_h0(sa, ca, sb, cb, rr[k], th0[k], th1[k], th2[k]);
+            }
             cw[k] = s0 ^ fl;
             // post-flip unsatisfied bonds (energy) and spins up, counted at once
             if constexpr (ACC_E) {
-                uint32_t v[NLV];
-#pragma unroll
-                for (int l = 0; l < NLV; ++l) v[l] = ecb[(k * NLV + l) * BTS];
-                vc_add_site<NLV>(v, sa ^ fl, sb ^ fl, ca ^ fl, cb ^ fl);
-#pragma unroll
-                for (int l = 0; l < NLV; ++l) ecb[(k * NLV + l) * BTS] = v[l];
+                wd[k][0] = sa ^ fl;
+                wd[k][1] = sb ^ fl;
+                wd[k][2] = ca ^ fl;
+                wd[k][3] = cb ^ fl;
             }
             if constexpr (ACC_M) {
                 uint32_t carry = cw[k];
@@ -203,10 +201,27 @@ __global__ void __launch_bounds__(colour_threads<ACC_E || ACC_M>()) stream_colou
         }
         Sc[n] = make_uint4(cw[0], cw[1], cw[2], cw[3]);
     };
-    // one site at a time: two per iteration (more registers, fewer resident
-    // blocks) measured slower at L=48
+    // sites in pairs: the energy counters take both at once (fewer counter
+    // updates); the two updates themselves run one after the other
+    static_assert(SPT % 2 == 0, "sites are counted in pairs");
 #pragma unroll 1
-    for (int m = 0; m < SPT; ++m) update_site(n_base + m * BT);
+    for (int m = 0; m < SPT; m += 2) {
+        uint32_t wa[4][4] = {}, wb[4][4] = {};
+        update_site(n_base + m * BT, wa);
+        update_site(n_base + (m + 1) * BT, wb);
+        if constexpr (ACC_E) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                uint32_t v[NLV];
+#pragma unroll
+                for (int l = 0; l < NLV; ++l) v[l] = ecb[(k * NLV + l) * BTS];
+                vc_add_2sites<NLV>(v, wa[k][0], wa[k][1], wa[k][2], wa[k][3], wb[k][0], wb[k][1],
+                                   wb[k][2], wb[k][3]);
+#pragma unroll
+                for (int l = 0; l < NLV; ++l) ecb[(k * NLV + l) * BTS] = v[l];
+            }
+        }
+    }
     __shared__ int sred[2][4][32];
     if (ACC_E || ACC_M) {
         uint32_t ecnt[4][NLV], mcnt[4][NLM];
