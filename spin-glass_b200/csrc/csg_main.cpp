@@ -193,10 +193,14 @@ int main(int argc, char** argv) {
         const size_t nrec = (size_t)st.ndis * st.nrep * 11;
         std::vector<float> rec(nrec);
         const auto t0 = std::chrono::steady_clock::now();
+        // csg_run only queues the section on the GPU: the next section is
+        // queued as soon as this one's records are taken, so that writing them
+        // to the file overlaps the GPU's work
+        check(csg_run(e, st.sbmeas), "run");
         for (int64_t done = 0; done < st.spfile; done += st.sbmeas) {
             log.progress(100.0 * (double)done / (double)st.spfile);
-            check(csg_run(e, st.sbmeas), "run");
             check(csg_obs_records(e, rec.data(), nrec), "observables");
+            if (done + st.sbmeas < st.spfile) check(csg_run(e, st.sbmeas), "run");
             out.write(reinterpret_cast<const char*>(rec.data()), (std::streamsize)(nrec * 4));
             if (!out) throw Error("write to " + base + "obs.bin failed");
         }
