@@ -3,12 +3,15 @@
 //
 // One sweep = two colour launches (stream_colour_kernel), then, when the
 // schedule asks for it, the exchange decisions (stream_decide_kernel), the
-// masked exchange (stream_exchange_kernel) and the overlap measurement
-// (stream_overlap_kernel + stream_measure_kernel).  The arithmetic of a site
-// update, of the energies and of the exchange rule is the same as the
-// cluster-resident kernel's (pt_kernel.cuh), so results are bit-identical to
-// it and to the CPU oracle.  Per-block partial sums (no atomics on the sweep
-// path) are reduced by the decision and measurement kernels.
+// masked exchange and the overlap counts in one pass
+// (stream_exchange_overlap_kernel; stream_exchange_kernel or
+// stream_overlap_kernel when only one of them is due) and the measurement
+// (stream_measure_kernel).  The arithmetic of a site update, of the energies
+// and of the exchange rule is the same as the cluster-resident kernel's
+// (pt_kernel.cuh), so results are bit-identical to it and to the CPU oracle.
+// Blocks add their counts to per-plane totals with integer atomics (any order
+// gives the same sums); the kernel that reads a total clears it.  The kernels
+// are launched with programmatic dependent launch (pdl_enter).
 #pragma once
 #include <cstdint>
 #include <type_traits>
@@ -22,9 +25,9 @@ namespace csg {
 // kStreamThreads threads, kStreamSPT sites of the colour per thread.
 constexpr int kStreamThreads = 256;
 constexpr int kStreamSPT = 8;
-// Colour launches that count (energies, magnetisations) hold more registers
-// (the bit-sliced counters grow with the sites per thread); their partial sums
-// are per block of kStreamAccSitesPerBlock sites.
+// Colour launches that count (energies, magnetisations) run smaller blocks of
+// kStreamAccSitesPerBlock sites (their counters live in shared memory, one
+// column per thread).
 constexpr int kStreamAccThreads = 128;
 constexpr int kStreamAccSPT = 8;
 constexpr int kStreamAccSitesPerBlock = kStreamAccThreads * kStreamAccSPT;
@@ -52,8 +55,8 @@ struct StreamParams {
     int* magn;    // [W][C][T][32]
     uint32_t* masks;  // [W][C][T] accepted-sample masks of the current round
     int L, W, C, T, Q;
-    int nblk;   // blocks per quad and colour
-    int nblk2;  // blocks per quad for the overlap (over all N sites)
+    int nblk;   // blocks per quad of a counting colour launch
+    int nblk2;  // blocks per quad of an overlap pass (over all N sites)
     uint32_t k0, k1, word0;
     uint32_t mag_plane;  // ceil(2^32 / (L*L/2)): division by multiply-high
     uint32_t mag_row;    // ceil(2^32 / (L/2))
@@ -357,8 +360,8 @@ __global__ void stream_exchange_kernel(const __grid_constant__ StreamParams P, i
 // 4 sites of both copies and walks the quads in order; on odd rounds quad q is
 // final only after its pair (3 of q, 0 of q+1) is exchanged, so each quad is
 // written (and its overlap counted) one step after it is loaded.  Every word
-// is read and written by exactly one thread.  Partial overlap counts go to
-// d_acc, like stream_overlap_kernel's.
+// is read and written by exactly one thread.  The block's overlap counts are
+// added to d_acc, as in stream_overlap_kernel.
 __global__ void __launch_bounds__(kStreamThreads) stream_exchange_overlap_kernel(
     const __grid_constant__ StreamParams P, int par) {
     pdl_enter();
@@ -441,8 +444,8 @@ __global__ void __launch_bounds__(kStreamThreads) stream_exchange_overlap_kernel
     }
 }
 
-// Overlap partial sums: blockIdx.x = (w, q), blockIdx.y = block of sites;
-// each thread kOverlapSPT sites.
+// Overlap counts: blockIdx.x = (w, q), blockIdx.y = block of sites; each
+// thread kOverlapSPT sites; the block's counts are added to d_acc.
 __global__ void __launch_bounds__(kStreamThreads) stream_overlap_kernel(const __grid_constant__ StreamParams P) {
     pdl_enter();
     const long N = (long)P.L * P.L * P.L;
@@ -488,9 +491,9 @@ __global__ void __launch_bounds__(kStreamThreads) stream_overlap_kernel(const __
     }
 }
 
-// Measurement accumulators from the energies and the overlap partials:
+// Measurement accumulators from the energies and the overlap totals:
 // blockIdx.x = (word, temperature), thread = (copy, sample); the first 32
-// threads also total the overlap partials of the plane.
+// threads also take (and clear) the plane's overlap totals.
 __global__ void stream_measure_kernel(const __grid_constant__ StreamParams P, bool need_M,
                                       StreamObs O) {
     pdl_enter();
