@@ -92,4 +92,42 @@ __global__ void measure_kernel(const uint32_t* __restrict__ spins, const uint32_
     for (int k = 0; k < 3 * L; ++k) dpl[(o * 3 * L) + k] = cnt[k * 32 + lane];
 }
 
+// The reference records (obs_s: e[2], m[2], q_0, q_1_r[3], q_1_i[3]) of one
+// (sample, temperature) from the integers of measure_kernel, with the float
+// and double operations of the host formulas (eamsim.cu:320-325, 477-509) in
+// the same order; cosv/sinv hold cos(k a), sin(k a), k = 2 pi / L, computed on
+// the host.  Built without contraction (-fmad=false), the records equal the
+// host's bit for bit.
+__global__ void records_kernel(const int* __restrict__ e, const int* __restrict__ m,
+                               const int* __restrict__ d, const int* __restrict__ dpl,
+                               const double* __restrict__ cosv, const double* __restrict__ sinv,
+                               int L, int W, int T, float H, float* __restrict__ rec) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;  // (w, b, t), t fastest
+    if (i >= (long)W * 32 * T) return;
+    const int t = (int)(i % T);
+    const long sb = i / T;  // sample 32 w + b
+    const int w = (int)(sb >> 5), b = (int)(sb & 31);
+    const long long N = (long long)L * L * L;
+    float* o = rec + i * 11;
+    for (int c = 0; c < 2; ++c) {
+        const size_t k = (((size_t)w * 2 + c) * T + t) * 32 + b;
+        const float es = (float)(-e[k]);
+        const float ms = (float)m[k];
+        o[c] = -(es + H * ms) / (float)N;
+        o[2 + c] = ms / (float)N;
+    }
+    const size_t k = ((size_t)w * T + t) * 32 + b;
+    o[4] = (float)(N - 2 * (long long)d[k]) / (float)N;
+    for (int dir = 0; dir < 3; ++dir) {
+        double re = 0.0, im = 0.0;
+        for (int a = 0; a < L; ++a) {
+            const long long P = (long long)L * L - 2 * (long long)dpl[(k * 3 + dir) * L + a];
+            re += (double)P * cosv[a];
+            im += (double)P * sinv[a];
+        }
+        o[5 + dir] = (float)(re / (double)N);
+        o[8 + dir] = (float)(im / (double)N);
+    }
+}
+
 }  // namespace csg

@@ -525,6 +525,8 @@ struct csg_engine {
     uint64_t* boundary = nullptr;
     int64_t sweep = 0, n_meas = 0, swap_rounds = 0, swap_round0 = 0;
     int qc = 0;  // quads per CTA chosen by a batch's tuner (0: automatic plan)
+    // device scratch of csg_obs_records, allocated at its first call
+    char* rec_scratch = nullptr;
 };
 
 namespace {
@@ -547,7 +549,7 @@ int dalloc(T** p, size_t n) {
 void free_engine(csg_engine* e) {
     void* ptrs[] = {e->spins, e->bonds, e->e_sum, e->m_sum, e->q_sum, e->q2_sum, e->q4_sum,
                     e->hist, e->e_last, e->m_last, e->d_last, e->swap_acc, e->swap_log,
-                    e->boundary};
+                    e->boundary, e->rec_scratch};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -840,63 +842,48 @@ int csg_obs_records(csg_engine* e, float* rec, size_t n_floats) {
     const size_t need = (size_t)32 * W * T * 11;
     if (n_floats != need) return fail(CSG_ERR_ARG, "record buffer size mismatch");
     const size_t nE = (size_t)W * 2 * T * 32, nD = (size_t)W * T * 32, nP = nD * 3 * L;
-    int *de = nullptr, *dm = nullptr, *dd = nullptr, *dp = nullptr;
-    int rc = dalloc(&de, nE);
-    if (!rc) rc = dalloc(&dm, nE);
-    if (!rc) rc = dalloc(&dd, nD);
-    if (!rc) rc = dalloc(&dp, nP);
-    std::vector<int> he(nE), hm(nE), hd(nD), hp(nP);
-    if (!rc) {
-        // 3L counters per lane; as many warps as fit in 48 KB (4 up to L = 32)
-        const size_t per_warp = (size_t)32 * 3 * L * sizeof(int);
-        const int warps = (int)std::max<size_t>(1, std::min<size_t>(4, 49152 / per_warp));
-        const unsigned blocks = (unsigned)((W * T + warps - 1) / warps);
-        const size_t sh = (size_t)warps * per_warp;
-        csg::measure_kernel<<<blocks, warps * 32, sh, e->stream>>>(e->spins, e->bonds, L, W, T, de,
-                                                                   dm, dd, dp);
-        cudaError_t ce = cudaGetLastError();
-        if (ce == cudaSuccess) ce = cudaMemcpyAsync(he.data(), de, nE * 4, cudaMemcpyDeviceToHost, e->stream);
-        if (ce == cudaSuccess) ce = cudaMemcpyAsync(hm.data(), dm, nE * 4, cudaMemcpyDeviceToHost, e->stream);
-        if (ce == cudaSuccess) ce = cudaMemcpyAsync(hd.data(), dd, nD * 4, cudaMemcpyDeviceToHost, e->stream);
-        if (ce == cudaSuccess) ce = cudaMemcpyAsync(hp.data(), dp, nP * 4, cudaMemcpyDeviceToHost, e->stream);
-        if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
-        if (ce != cudaSuccess) rc = fail(CSG_ERR_CUDA, std::string("measure: ") + cudaGetErrorString(ce));
+    // scratch: integers, the phase tables, the records
+    const size_t o_m = nE * 4, o_d = o_m + nE * 4, o_p = o_d + nD * 4, o_cs = (o_p + nP * 4 + 15) & ~(size_t)15;
+    const size_t o_rec = o_cs + (size_t)2 * L * 8, bytes = o_rec + need * 4;
+    if (!e->rec_scratch) {
+        const cudaError_t ce = cudaMalloc(reinterpret_cast<void**>(&e->rec_scratch), bytes);
+        if (ce != cudaSuccess) {
+            cudaGetLastError();
+            e->rec_scratch = nullptr;
+            return fail(CSG_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(ce));
+        }
     }
-    for (void* p : {(void*)de, (void*)dm, (void*)dd, (void*)dp})
-        if (p) cudaFree(p);
-    if (rc) return rc;
-    const int64_t N = (int64_t)L * L * L;
-    const float H = (float)e->cfg.H;
+    char* sc = e->rec_scratch;
+    int* de = reinterpret_cast<int*>(sc);
+    int* dm = reinterpret_cast<int*>(sc + o_m);
+    int* dd = reinterpret_cast<int*>(sc + o_d);
+    int* dp = reinterpret_cast<int*>(sc + o_p);
+    double* dcs = reinterpret_cast<double*>(sc + o_cs);
+    float* drec = reinterpret_cast<float*>(sc + o_rec);
+    // the L phases exp(i k a), k = 2 pi / L, computed on the host
     const double k = 2.0 * M_PI / L;
-    std::vector<double> cosv(L), sinv(L);  // the L phases exp(i k a), computed once
+    std::vector<double> cs(2 * (size_t)L);
     for (int a = 0; a < L; ++a) {
-        cosv[a] = std::cos(k * a);
-        sinv[a] = std::sin(k * a);
+        cs[a] = std::cos(k * a);
+        cs[L + a] = std::sin(k * a);
     }
-    for (int w = 0; w < W; ++w)
-        for (int b = 0; b < 32; ++b)
-            for (int t = 0; t < T; ++t) {
-                float* o = rec + (((size_t)(32 * w + b)) * T + t) * 11;
-                for (int c = 0; c < 2; ++c) {
-                    const size_t i = (((size_t)w * 2 + c) * T + t) * 32 + b;
-                    const float es = (float)(-he[i]);
-                    const float ms = (float)hm[i];
-                    o[c] = -(es + H * ms) / (float)N;
-                    o[2 + c] = ms / (float)N;
-                }
-                const size_t i = ((size_t)w * T + t) * 32 + b;
-                o[4] = (float)(N - 2 * (int64_t)hd[i]) / (float)N;
-                for (int dir = 0; dir < 3; ++dir) {
-                    double re = 0.0, im = 0.0;
-                    for (int a = 0; a < L; ++a) {
-                        const int64_t P = (int64_t)L * L - 2 * (int64_t)hp[(i * 3 + dir) * L + a];
-                        re += (double)P * cosv[a];
-                        im += (double)P * sinv[a];
-                    }
-                    o[5 + dir] = (float)(re / (double)N);
-                    o[8 + dir] = (float)(im / (double)N);
-                }
-            }
+    // 3L counters per lane; as many warps as fit in 48 KB (4 up to L = 32)
+    const size_t per_warp = (size_t)32 * 3 * L * sizeof(int);
+    const int warps = (int)std::max<size_t>(1, std::min<size_t>(4, 49152 / per_warp));
+    const unsigned blocks = (unsigned)((W * T + warps - 1) / warps);
+    const size_t sh = (size_t)warps * per_warp;
+    cudaError_t ce = cudaMemcpyAsync(dcs, cs.data(), cs.size() * 8, cudaMemcpyHostToDevice, e->stream);
+    if (ce == cudaSuccess) {
+        csg::measure_kernel<<<blocks, warps * 32, sh, e->stream>>>(e->spins, e->bonds, L, W, T, de, dm,
+                                                                   dd, dp);
+        const long total = (long)W * 32 * T;
+        csg::records_kernel<<<(unsigned)((total + 127) / 128), 128, 0, e->stream>>>(
+            de, dm, dd, dp, dcs, dcs + L, L, W, T, (float)e->cfg.H, drec);
+        ce = cudaGetLastError();
+    }
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(rec, drec, need * 4, cudaMemcpyDeviceToHost, e->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    if (ce != cudaSuccess) return fail(CSG_ERR_CUDA, std::string("records: ") + cudaGetErrorString(ce));
     return CSG_OK;
 }
 
