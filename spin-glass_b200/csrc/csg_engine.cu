@@ -1016,10 +1016,22 @@ int capture(csg_batch* b, int64_t n_sweeps, bool with_obs, cudaGraphExec_t* out)
     std::vector<Plan> plans(b->eng.size());
     for (size_t i = 0; i < b->eng.size(); ++i)
         if (int rc = plan_member(b->eng[i], plans[i], b->spread)) return rc;
+    // Branches in order of decreasing cluster size (then shared memory per CTA):
+    // the GPU places the clusters of the first branches first, and putting the
+    // largest first packs the GPCs best (best-fit decreasing).  On the mixed
+    // L=12/14/16 workload this order measured up to 36 % faster than member
+    // order.
+    std::vector<size_t> order(b->eng.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) {
+        if (plans[x].K != plans[y].K) return plans[x].K > plans[y].K;
+        return plans[x].smem > plans[y].smem;
+    });
     CSG_CUDA(cudaStreamBeginCapture(b->main, cudaStreamCaptureModeThreadLocal));
     int rc = CSG_OK;
     cudaError_t ce = cudaEventRecord(b->fork, b->main);
-    for (size_t i = 0; i < b->eng.size() && rc == CSG_OK && ce == cudaSuccess; ++i) {
+    for (size_t oi = 0; oi < order.size() && rc == CSG_OK && ce == cudaSuccess; ++oi) {
+        const size_t i = order[oi];
         csg_engine* e = b->eng[i];
         ce = cudaStreamWaitEvent(e->stream, b->fork, 0);
         if (ce != cudaSuccess) break;
