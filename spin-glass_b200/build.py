@@ -21,8 +21,10 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
           "-ffp-contract=off", "-fmad=false", f"-I{ROOT / 'include'}", f"-I{CSRC}"]
 
-LIB_SOURCES = [CSRC / "csg_engine.cu", CSRC / "obs_noalloc.cu", CSRC / "analysis_kernels.cu"]
-LIB_DEPS = LIB_SOURCES + sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "csg.h"]
+LIB_SOURCES = [CSRC / "csg_engine.cu", CSRC / "batch.cpp", CSRC / "server.cpp",
+               CSRC / "obs_noalloc.cu", CSRC / "analysis_kernels.cu"]
+LIB_DEPS = (LIB_SOURCES + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h"))
+            + [ROOT / "include" / "csg.h"])
 CLI_SOURCES = [CSRC / "csg_main.cpp"]
 
 

@@ -13,17 +13,11 @@
 #include <vector>
 
 #include "csg.h"
+#include "engine_internal.h"
 
-namespace csg_detail {
-void set_last_error(const std::string& msg);  // csg_engine.cu (not exported)
-}
+using csg_detail::fail;  // reported by csg_last_error()
 
 namespace {
-
-int fail(int code, const std::string& msg) {
-    csg_detail::set_last_error(msg);
-    return code;
-}
 
 constexpr int kRecFloats = 11;  // obs_s: e[2], m[2], q_0, q_1_r[3], q_1_i[3]
 constexpr int kSums = 9;        // q_0^2, q_1_r[a]^2 (3), q_1_i[a]^2 (3), e (both copies), m

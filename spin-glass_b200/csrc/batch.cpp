@@ -1,0 +1,327 @@
+// batch.cpp — the batched engine: several simulations (any mix of L, samples,
+// ladders) run as parallel branches of one captured CUDA graph, so that their
+// clusters share the SMs that any single one leaves idle.  Each member keeps
+// its own Philox counters, so its results do not depend on the batch it runs
+// in.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <new>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "csg.h"
+#include "engine_internal.h"
+
+using namespace csg_detail;
+
+struct csg_batch {
+    std::vector<csg_engine*> eng;
+    cudaStream_t main = nullptr;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
+    long long* counters = nullptr;  // device sweep counter per member
+    std::vector<std::pair<int64_t, cudaGraphExec_t>> graphs;
+    // pad every member CTA's shared memory past half an SM, so that no two
+    // CTAs share an SM (chosen by the tuner)
+    bool spread = false;
+};
+
+namespace {
+
+void drop_graphs(csg_batch* b) {
+    for (auto& g : b->graphs) cudaGraphExecDestroy(g.second);
+    b->graphs.clear();
+}
+
+// more than half of an SM's 228 KB (with the 1 KB per-CTA reserve)
+constexpr size_t kSpreadSmem = 116 * 1024;
+
+int capture(csg_batch* b, int64_t n_sweeps, bool with_obs, cudaGraphExec_t* out) {
+    std::vector<Plan> plans(b->eng.size());
+    for (size_t i = 0; i < b->eng.size(); ++i)
+        if (int rc = plan_engine(b->eng[i], plans[i], b->spread ? kSpreadSmem : 0)) return rc;
+    // Branches in order of decreasing cluster size (then shared memory per CTA):
+    // the GPU places the clusters of the first branches first, and putting the
+    // largest first packs the GPCs best (best-fit decreasing).  On the mixed
+    // L=12/14/16 workload this order measured up to 36 % faster than member
+    // order.
+    std::vector<size_t> order(b->eng.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) {
+        if (plans[x].K != plans[y].K) return plans[x].K > plans[y].K;
+        return plans[x].smem > plans[y].smem;
+    });
+    CSG_CUDA(cudaStreamBeginCapture(b->main, cudaStreamCaptureModeThreadLocal));
+    int rc = CSG_OK;
+    cudaError_t ce = cudaEventRecord(b->fork, b->main);
+    for (size_t oi = 0; oi < order.size() && rc == CSG_OK && ce == cudaSuccess; ++oi) {
+        const size_t i = order[oi];
+        csg_engine* e = b->eng[i];
+        ce = cudaStreamWaitEvent(e->stream, b->fork, 0);
+        if (ce != cudaSuccess) break;
+        const csg_device_obs o = device_obs(e);
+        rc = run_device(e->cfg, e->spins, e->bonds, with_obs ? &o : nullptr, 0, n_sweeps, e->stream,
+                        0, b->counters + i, &plans[i]);
+        if (rc == CSG_OK) ce = cudaEventRecord(b->join[i], e->stream);
+        if (ce == cudaSuccess) ce = cudaStreamWaitEvent(b->main, b->join[i], 0);
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce2 = cudaStreamEndCapture(b->main, &g);
+    if (rc != CSG_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (ce != cudaSuccess || ce2 != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return fail(CSG_ERR_CUDA, std::string("graph capture: ") +
+                                      cudaGetErrorString(ce != cudaSuccess ? ce : ce2));
+    }
+    const cudaError_t ce3 = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (ce3 != cudaSuccess)
+        return fail(CSG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce3));
+    return CSG_OK;
+}
+
+// Launch the batch graph for n sweeps from the members' host sweep counters.
+int launch_batch(csg_batch* b, int64_t n_sweeps, bool with_obs) {
+    for (csg_engine* e : b->eng) CSG_CUDA(cudaStreamSynchronize(e->stream));
+    cudaGraphExec_t exec = nullptr;
+    if (with_obs)
+        for (auto& g : b->graphs)
+            if (g.first == n_sweeps) exec = g.second;
+    if (!exec) {
+        if (int rc = capture(b, n_sweeps, with_obs, &exec)) return rc;
+        if (with_obs) b->graphs.push_back({n_sweeps, exec});
+    }
+    std::vector<long long> start(b->eng.size());
+    for (size_t i = 0; i < b->eng.size(); ++i) start[i] = b->eng[i]->sweep;
+    CSG_CUDA(cudaMemcpyAsync(b->counters, start.data(), start.size() * sizeof(long long),
+                             cudaMemcpyHostToDevice, b->main));
+    CSG_CUDA(cudaGraphLaunch(exec, b->main));
+    if (!with_obs) {
+        CSG_CUDA(cudaStreamSynchronize(b->main));
+        cudaGraphExecDestroy(exec);
+    }
+    return CSG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int csg_batch_create(const csg_config* cfgs, int32_t n, csg_batch** out) {
+    if (!out || !cfgs || n < 1) return fail(CSG_ERR_ARG, "bad batch arguments");
+    *out = nullptr;
+    csg_batch* b = new (std::nothrow) csg_batch();
+    if (!b) return fail(CSG_ERR_NOMEM, "host allocation failed");
+    int rc = CSG_OK;
+    for (int i = 0; i < n && rc == CSG_OK; ++i) {
+        csg_engine* e = nullptr;
+        rc = csg_engine_create(&cfgs[i], &e);
+        if (rc == CSG_OK && use_stream(cfgs[i])) {
+            csg_engine_destroy(e);
+            rc = fail(CSG_ERR_UNSUPPORTED,
+                      "batch members need the cluster-resident kernel (L <= 24, no CSG_ENGINE_STREAM)");
+        }
+        if (rc == CSG_OK) b->eng.push_back(e);
+    }
+    if (rc == CSG_OK && cudaStreamCreateWithFlags(&b->main, cudaStreamNonBlocking) != cudaSuccess)
+        rc = fail(CSG_ERR_CUDA, "cudaStreamCreate failed");
+    if (rc == CSG_OK && cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess)
+        rc = fail(CSG_ERR_CUDA, "cudaEventCreate failed");
+    for (int i = 0; i < n && rc == CSG_OK; ++i) {
+        cudaEvent_t ev;
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
+            rc = fail(CSG_ERR_CUDA, "cudaEventCreate failed");
+        else
+            b->join.push_back(ev);
+    }
+    if (rc == CSG_OK) rc = dalloc(&b->counters, (size_t)n);
+    if (rc != CSG_OK) {
+        const std::string msg = last_error();
+        csg_batch_destroy(b);
+        set_last_error(msg);
+        return rc;
+    }
+    *out = b;
+    return CSG_OK;
+}
+
+int csg_batch_destroy(csg_batch* b) {
+    if (!b) return CSG_OK;
+    if (b->main) cudaStreamSynchronize(b->main);
+    drop_graphs(b);
+    for (csg_engine* e : b->eng) csg_engine_destroy(e);
+    for (cudaEvent_t ev : b->join) cudaEventDestroy(ev);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->main) cudaStreamDestroy(b->main);
+    if (b->counters) cudaFree(b->counters);
+    delete b;
+    return CSG_OK;
+}
+
+int csg_batch_engine(csg_batch* b, int32_t i, csg_engine** out) {
+    if (!b || !out || i < 0 || i >= (int32_t)b->eng.size()) return fail(CSG_ERR_ARG, "bad member index");
+    *out = b->eng[i];
+    return CSG_OK;
+}
+
+int csg_batch_run(csg_batch* b, int64_t n_sweeps) {
+    if (!b || n_sweeps < 0) return fail(CSG_ERR_ARG, "bad batch run arguments");
+    if (n_sweeps == 0) return CSG_OK;
+    if (int rc = launch_batch(b, n_sweeps, true)) return rc;
+    CSG_CUDA(cudaStreamSynchronize(b->main));
+    for (csg_engine* e : b->eng) account(e, n_sweeps);
+    return CSG_OK;
+}
+
+int csg_batch_run_sequential(csg_batch* b, int64_t n_sweeps) {
+    if (!b || n_sweeps < 0) return fail(CSG_ERR_ARG, "bad batch run arguments");
+    for (csg_engine* e : b->eng) CSG_CUDA(cudaStreamSynchronize(e->stream));
+    for (csg_engine* e : b->eng) {
+        const csg_device_obs o = device_obs(e);
+        if (int rc = run_device(e->cfg, e->spins, e->bonds, &o, e->sweep, n_sweeps, b->main, e->qc))
+            return rc;
+        account(e, n_sweeps);
+    }
+    CSG_CUDA(cudaStreamSynchronize(b->main));
+    return CSG_OK;
+}
+
+int csg_batch_set_plan(csg_batch* b, const int32_t* quads_per_cta) {
+    if (!b || !quads_per_cta) return fail(CSG_ERR_ARG, "null argument");
+    for (size_t i = 0; i < b->eng.size(); ++i) {
+        const csg_dims& d = b->eng[i]->cfg.dims;
+        const int G = d.n_copies * d.n_temps / 4;
+        if (quads_per_cta[i] < 0 || (quads_per_cta[i] > 0 && G % quads_per_cta[i]))
+            return fail(CSG_ERR_ARG, "quads_per_cta must divide n_copies*n_temps/4");
+    }
+    for (size_t i = 0; i < b->eng.size(); ++i) b->eng[i]->qc = quads_per_cta[i];
+    drop_graphs(b);
+    return CSG_OK;
+}
+
+// Autotuner: times the whole batch graph for probe_sweeps sweeps (best of two)
+// for every combination of the members' quads per CTA, each with and without
+// one SM per CTA, when there are at most 256 such combinations; otherwise
+// coordinate descent over one member at a time
+// with the others fixed (two passes).  The members' spins are saved before and restored
+// after, and the probes accumulate no observables, so tuning leaves the
+// simulations exactly as they were.
+int csg_batch_tune(csg_batch* b, int64_t probe_sweeps, int32_t* chosen) {
+    if (!b || probe_sweeps < 1) return fail(CSG_ERR_ARG, "bad tune arguments");
+    const size_t n = b->eng.size();
+    std::vector<uint32_t*> saved(n, nullptr);
+    int rc = CSG_OK;
+    for (size_t i = 0; i < n && rc == CSG_OK; ++i) {
+        rc = dalloc(&saved[i], b->eng[i]->n_spins);
+        if (rc == CSG_OK)
+            if (cudaMemcpyAsync(saved[i], b->eng[i]->spins, b->eng[i]->n_spins * 4,
+                                cudaMemcpyDeviceToDevice, b->eng[i]->stream) != cudaSuccess)
+                rc = fail(CSG_ERR_CUDA, "snapshot copy failed");
+    }
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    if (rc == CSG_OK && (cudaEventCreate(&t0) != cudaSuccess || cudaEventCreate(&t1) != cudaSuccess))
+        rc = fail(CSG_ERR_CUDA, "cudaEventCreate failed");
+    auto time_batch = [&](float& ms_out) -> int {
+        cudaGraphExec_t exec = nullptr;
+        if (int r = capture(b, probe_sweeps, false, &exec)) return r;
+        float best = 1e30f;
+        for (int rep = 0; rep < 3; ++rep) {  // first launch warms up
+            std::vector<long long> start(n, 0);
+            CSG_CUDA(cudaMemcpyAsync(b->counters, start.data(), n * sizeof(long long),
+                                     cudaMemcpyHostToDevice, b->main));
+            CSG_CUDA(cudaEventRecord(t0, b->main));
+            CSG_CUDA(cudaGraphLaunch(exec, b->main));
+            CSG_CUDA(cudaEventRecord(t1, b->main));
+            CSG_CUDA(cudaEventSynchronize(t1));
+            float ms = 0.f;
+            CSG_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+            if (rep > 0 && ms < best) best = ms;
+        }
+        cudaGraphExecDestroy(exec);
+        ms_out = best;
+        return CSG_OK;
+    };
+    for (size_t i = 0; i < n && rc == CSG_OK; ++i) {
+        Plan pl;
+        rc = plan_engine(b->eng[i], pl);  // start from the per-member plan
+        if (rc == CSG_OK) b->eng[i]->qc = pl.Qc;
+    }
+    // the quads-per-CTA values each member can take
+    std::vector<std::vector<int>> options(n);
+    size_t combos = 1;
+    for (size_t i = 0; i < n; ++i) {
+        options[i] = quad_splits(b->eng[i]->cfg);
+        combos *= std::max<size_t>(1, options[i].size());
+    }
+    if (2 * combos <= 256) {
+        // few enough combinations: time every one, with and without one SM per
+        // CTA (members share the GPU, so the best plan of one member depends
+        // on the others')
+        float best_ms = 1e30f;
+        bool best_spread = false;
+        std::vector<int> best(n);
+        for (size_t i = 0; i < n; ++i) best[i] = b->eng[i]->qc;
+        for (size_t k = 0; k < 2 * combos && rc == CSG_OK; ++k) {
+            b->spread = k >= combos;
+            size_t r = k % combos;
+            for (size_t i = 0; i < n; ++i) {
+                const size_t m = options[i].size();
+                if (m) b->eng[i]->qc = options[i][r % m];
+                r /= std::max<size_t>(1, m);
+            }
+            float ms = 0.f;
+            if (time_batch(ms) != CSG_OK) {  // e.g. a cluster shape the device cannot place
+                cudaGetLastError();
+                continue;
+            }
+            if (ms < best_ms) {
+                best_ms = ms;
+                best_spread = b->spread;
+                for (size_t i = 0; i < n; ++i) best[i] = b->eng[i]->qc;
+            }
+        }
+        for (size_t i = 0; i < n; ++i) b->eng[i]->qc = best[i];
+        b->spread = best_spread;
+    }
+    for (int pass = 0; pass < 2 && rc == CSG_OK && 2 * combos > 256; ++pass)
+        for (size_t i = 0; i < n && rc == CSG_OK; ++i) {
+            csg_engine* e = b->eng[i];
+            int best_qc = e->qc;
+            float best_ms = 1e30f;
+            for (const int qc : options[i]) {
+                e->qc = qc;
+                float ms = 0.f;
+                const int r = time_batch(ms);
+                if (r != CSG_OK) {  // e.g. a cluster shape the device cannot place
+                    cudaGetLastError();
+                    continue;
+                }
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best_qc = qc;
+                }
+            }
+            e->qc = best_qc;
+        }
+    for (size_t i = 0; i < n; ++i) {
+        if (saved[i]) {
+            if (rc == CSG_OK &&
+                cudaMemcpy(b->eng[i]->spins, saved[i], b->eng[i]->n_spins * 4,
+                           cudaMemcpyDeviceToDevice) != cudaSuccess)
+                rc = fail(CSG_ERR_CUDA, "restore copy failed");
+            cudaFree(saved[i]);
+        }
+        if (chosen) chosen[i] = b->eng[i]->qc;
+    }
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
+    drop_graphs(b);
+    return rc;
+}
+
+}  // extern "C"

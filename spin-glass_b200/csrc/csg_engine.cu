@@ -1,58 +1,60 @@
 // csg_engine.cu — host side of libcsg.so: configuration checks, acceptance
-// tables, launch planning and the C ABI declared in include/csg.h.
+// tables, launch planning, the sweep launches of both engines and the C ABI of
+// one engine (include/csg.h).  The batched engine is batch.cpp, the request
+// server server.cpp.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <new>
 #include <string>
 #include <utility>
 #include <vector>
 
 #include "csg.h"
+#include "engine_internal.h"
 #include "philox.cuh"
 #include "pt_kernel.cuh"
 #include "aux_kernels.cuh"
 #include "stream_kernels.cuh"
 
-namespace {
+namespace csg_detail {
 
+namespace {
 thread_local std::string g_err;
+}  // namespace
 
 int fail(int code, const std::string& msg) {
     g_err = msg;
     return code;
 }
 
-}  // namespace
+void set_last_error(const std::string& msg) { g_err = msg; }
 
-// Lets other translation units of the library report through csg_last_error().
-namespace csg_detail {
-__attribute__((visibility("hidden"))) void set_last_error(const std::string& msg) { g_err = msg; }
+const std::string& last_error() { return g_err; }
+
 }  // namespace csg_detail
 
-namespace {
+using namespace csg_detail;
 
-#define CSG_CUDA(call)                                                                    \
-    do {                                                                                  \
-        const cudaError_t e_ = (call);                                                    \
-        if (e_ != cudaSuccess)                                                            \
-            return fail(CSG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
-    } while (0)
+namespace {
 
 constexpr int kMaxResidentL = 24;  // largest L of the cluster-resident kernel
 constexpr int kMaxL = 128;         // largest L of the streaming engine
 
 bool lattice_supported(int L) { return L >= 4 && L <= kMaxL && L % 2 == 0; }
 
+}  // namespace
+
 // Lattices whose quads do not fit in a cluster's shared memory run on the
 // streaming engine; CSG_ENGINE_STREAM selects it for any L.
-bool use_stream(const csg_config& c) {
+bool csg_detail::use_stream(const csg_config& c) {
     return c.dims.L > kMaxResidentL || (c.flags & CSG_ENGINE_STREAM);
 }
 
-int validate(const csg_config* cfg) {
+int csg_detail::validate(const csg_config* cfg) {
     if (!cfg) return fail(CSG_ERR_ARG, "null configuration");
     const csg_dims& d = cfg->dims;
     if (d.L < 4 || d.L % 2 != 0) return fail(CSG_ERR_ARG, "L must be even and >= 4");
@@ -74,6 +76,8 @@ int validate(const csg_config* cfg) {
     if (cfg->word0 < 0) return fail(CSG_ERR_ARG, "negative word0");
     return CSG_OK;
 }
+
+namespace {
 
 // Acceptance table: for centre spin bit s and U unsatisfied bonds the energy
 // change of a flip is dE = 12 - 4U + 2H(2s-1); the flip is accepted when a
@@ -153,11 +157,6 @@ size_t smem_for(int L, int Qc, bool has_m, bool gen) {
 }
 
 constexpr size_t kMaxSmem = 227 * 1024;
-
-struct Plan {
-    int Qc = 0, K = 0, TPQ = 0;
-    size_t smem = 0;
-};
 
 std::mutex g_plan_mu;
 csg_plan g_override = {0, 0, 0, 0};
@@ -450,9 +449,12 @@ int run_stream(const csg_config& cfg, uint32_t* spins, const uint32_t* bonds,
     return CSG_OK;
 }
 
-int run_device(const csg_config& cfg, uint32_t* spins, const uint32_t* bonds,
-               const csg_device_obs* obs, int64_t sweep0, int64_t n_sweeps, cudaStream_t st,
-               int forced_qc = 0, long long* sweep_dev = nullptr, const Plan* plan_in = nullptr) {
+}  // namespace
+
+int csg_detail::run_device(const csg_config& cfg, uint32_t* spins, const uint32_t* bonds,
+                           const csg_device_obs* obs, int64_t sweep0, int64_t n_sweeps,
+                           cudaStream_t st, int forced_qc, long long* sweep_dev,
+                           const Plan* plan_in) {
     if (use_stream(cfg)) {
         if (sweep_dev)
             return fail(CSG_ERR_UNSUPPORTED, "the streaming engine takes no device sweep counter");
@@ -503,48 +505,76 @@ int run_device(const csg_config& cfg, uint32_t* spins, const uint32_t* bonds,
     return CSG_OK;
 }
 
-}  // namespace
+
+std::vector<int> csg_detail::quad_splits(const csg_config& c) {
+    std::vector<int> out;
+    if (use_stream(c)) return out;
+    csg::PtParams P;
+    bool gen = false;
+    fill_params(c, P, gen);
+    const int L = c.dims.L, G = c.dims.n_copies * c.dims.n_temps / 4;
+    const bool has_m = gen || (c.flags & CSG_MEASURE_M);
+    for (int qc = 1; qc <= G; ++qc)
+        if (G % qc == 0 && G / qc <= 16 && smem_for(L, qc, has_m, gen) <= kMaxSmem &&
+            qc * csg::tpq_for(L) <= csg::kMaxThreads)
+            out.push_back(qc);
+    return out;
+}
+
+int csg_detail::plan_engine(csg_engine* e, Plan& pl, size_t min_smem) {
+    csg::PtParams P;
+    bool gen = false;
+    fill_params(e->cfg, P, gen);
+    if (int rc = make_plan(e->cfg, gen, pl, e->qc)) return rc;
+    if (pl.smem < min_smem && !use_stream(e->cfg)) {
+        pl.smem = min_smem;
+        return prepare_kernel(select_kernel(e->cfg.dims.L, gen), pl.smem, pl.K);
+    }
+    return CSG_OK;
+}
+
+size_t csg_detail::footprint_bytes(const csg_config& c) {
+    const csg_dims& d = c.dims;
+    const size_t N = (size_t)d.L * d.L * d.L;
+    const size_t ne = (size_t)d.n_words * d.n_copies * d.n_temps * 32;
+    const size_t nq = d.n_copies == 2 ? (size_t)d.n_words * d.n_temps * 32 : 0;
+    const size_t nh = d.n_copies == 2 ? (size_t)d.n_temps * (N + 1) : 0;
+    return (size_t)d.n_words * d.n_copies * d.n_temps * N * 4 + (size_t)d.n_words * 3 * N * 4 +
+           ne * (8 + 8 + 4 + 4) + nq * (8 + 8 + 16 + 4) + nh * 4 +
+           (size_t)d.n_copies * d.n_temps * 8 + (size_t)c.swap_log_rounds * ne / 32 * 4 + 8 +
+           (use_stream(c) ? stream_layout(c).bytes : 0);
+}
+
+void csg_detail::account(csg_engine* e, int64_t n) {
+    const csg_schedule& sc = e->cfg.sched;
+    e->swap_rounds += count_events(e->sweep, n, sc.sweeps_per_swap, 0);
+    e->n_meas += count_events(e->sweep, n, sc.sweeps_per_meas, sc.meas_start);
+    e->sweep += n;
+}
+
+csg_device_obs csg_detail::device_obs(const csg_engine* e) {
+    csg_device_obs o{};
+    o.e_sum = e->e_sum;
+    o.m_sum = e->m_sum;
+    o.q_sum = e->q_sum;
+    o.q2_sum = e->q2_sum;
+    o.q4_sum = e->q4_sum;
+    o.hist = e->hist;
+    o.e_last = e->e_last;
+    o.m_last = e->m_last;
+    o.d_last = e->d_last;
+    o.swap_acc = e->swap_acc;
+    o.swap_log = e->swap_log;
+    o.swap_log_rounds = e->cfg.swap_log_rounds;
+    o.swap_round0 = e->swap_round0;
+    o.boundary = e->boundary;
+    return o;
+}
 
 // ---------------------------------------------------------------------------
 // Engine object
 // ---------------------------------------------------------------------------
-struct csg_engine {
-    csg_config cfg{};
-    std::vector<double> betas;
-    cudaStream_t stream = nullptr;
-    size_t n_spins = 0, n_bonds = 0, n_e = 0, n_q = 0, n_hist = 0;
-    uint32_t* spins = nullptr;
-    uint32_t* bonds = nullptr;
-    // device accumulators
-    int64_t *e_sum = nullptr, *m_sum = nullptr, *q_sum = nullptr, *q2_sum = nullptr;
-    uint64_t* q4_sum = nullptr;
-    uint32_t* hist = nullptr;
-    int32_t *e_last = nullptr, *m_last = nullptr, *d_last = nullptr;
-    uint64_t* swap_acc = nullptr;
-    uint32_t* swap_log = nullptr;
-    uint64_t* boundary = nullptr;
-    int64_t sweep = 0, n_meas = 0, swap_rounds = 0, swap_round0 = 0;
-    int qc = 0;  // quads per CTA chosen by a batch's tuner (0: automatic plan)
-    // device scratch of csg_obs_records, allocated at its first call
-    char* rec_scratch = nullptr;
-};
-
 namespace {
-
-template <typename T>
-int dalloc(T** p, size_t n) {
-    if (n == 0) {
-        *p = nullptr;
-        return CSG_OK;
-    }
-    const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T));
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        *p = nullptr;
-        return fail(CSG_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-    }
-    return CSG_OK;
-}
 
 void free_engine(csg_engine* e) {
     void* ptrs[] = {e->spins, e->bonds, e->e_sum, e->m_sum, e->q_sum, e->q2_sum, e->q4_sum,
@@ -574,30 +604,18 @@ int reset_obs(csg_engine* e) {
     return CSG_OK;
 }
 
-csg_device_obs device_obs(const csg_engine* e) {
-    csg_device_obs o{};
-    o.e_sum = e->e_sum;
-    o.m_sum = e->m_sum;
-    o.q_sum = e->q_sum;
-    o.q2_sum = e->q2_sum;
-    o.q4_sum = e->q4_sum;
-    o.hist = e->hist;
-    o.e_last = e->e_last;
-    o.m_last = e->m_last;
-    o.d_last = e->d_last;
-    o.swap_acc = e->swap_acc;
-    o.swap_log = e->swap_log;
-    o.swap_log_rounds = e->cfg.swap_log_rounds;
-    o.swap_round0 = e->swap_round0;
-    o.boundary = e->boundary;
-    return o;
-}
-
 }  // namespace
 
 extern "C" {
 
-const char* csg_last_error(void) { return g_err.c_str(); }
+const char* csg_last_error(void) { return last_error().c_str(); }
+
+int csg_engine_footprint(const csg_config* cfg, size_t* bytes) {
+    if (int rc = validate(cfg)) return rc;
+    if (!bytes) return fail(CSG_ERR_ARG, "null output");
+    *bytes = footprint_bytes(*cfg);
+    return CSG_OK;
+}
 
 int csg_engine_create(const csg_config* cfg, csg_engine** out) {
     if (!out) return fail(CSG_ERR_ARG, "null output pointer");
@@ -649,10 +667,10 @@ int csg_engine_create(const csg_config* cfg, csg_engine** out) {
         rc = make_plan(e->cfg, gen, pl);
     }
     if (rc != CSG_OK) {
-        const std::string msg = g_err;
+        const std::string msg = last_error();
         free_engine(e);
         delete e;
-        g_err = msg;
+        set_last_error(msg);
         return rc;
     }
     *out = e;
@@ -723,10 +741,7 @@ int csg_run(csg_engine* e, int64_t n_sweeps) {
     const csg_device_obs o = device_obs(e);
     if (int rc = run_device(e->cfg, e->spins, e->bonds, &o, e->sweep, n_sweeps, e->stream, e->qc))
         return rc;
-    const csg_schedule& sc = e->cfg.sched;
-    e->swap_rounds += count_events(e->sweep, n_sweeps, sc.sweeps_per_swap, 0);
-    e->n_meas += count_events(e->sweep, n_sweeps, sc.sweeps_per_meas, sc.meas_start);
-    e->sweep += n_sweeps;
+    account(e, n_sweeps);
     return CSG_OK;
 }
 
@@ -972,518 +987,3 @@ int csg_load_checkpoint(csg_engine* e, const uint32_t* ref, size_t n_words, int6
 
 }  // extern "C"
 
-// ---------------------------------------------------------------------------
-// Batched engine: several simulations (any mix of L, samples, ladders) run as
-// parallel branches of one captured CUDA graph, so that their clusters share
-// the SMs that any single one leaves idle.  Each member keeps its own Philox
-// counters, so its results do not depend on the batch it runs in.
-// ---------------------------------------------------------------------------
-struct csg_batch {
-    std::vector<csg_engine*> eng;
-    cudaStream_t main = nullptr;
-    cudaEvent_t fork = nullptr;
-    std::vector<cudaEvent_t> join;
-    long long* counters = nullptr;  // device sweep counter per member
-    std::vector<std::pair<int64_t, cudaGraphExec_t>> graphs;
-    // pad every member CTA's shared memory past half an SM, so that no two
-    // CTAs share an SM (chosen by the tuner)
-    bool spread = false;
-};
-
-namespace {
-
-void drop_graphs(csg_batch* b) {
-    for (auto& g : b->graphs) cudaGraphExecDestroy(g.second);
-    b->graphs.clear();
-}
-
-// more than half of an SM's 228 KB (with the 1 KB per-CTA reserve)
-constexpr size_t kSpreadSmem = 116 * 1024;
-
-int plan_member(csg_engine* e, Plan& pl, bool spread = false) {
-    csg::PtParams P;
-    bool gen = false;
-    fill_params(e->cfg, P, gen);
-    if (int rc = make_plan(e->cfg, gen, pl, e->qc)) return rc;
-    if (spread && pl.smem < kSpreadSmem) {
-        pl.smem = kSpreadSmem;
-        return prepare_kernel(select_kernel(e->cfg.dims.L, gen), pl.smem, pl.K);
-    }
-    return CSG_OK;
-}
-
-int capture(csg_batch* b, int64_t n_sweeps, bool with_obs, cudaGraphExec_t* out) {
-    std::vector<Plan> plans(b->eng.size());
-    for (size_t i = 0; i < b->eng.size(); ++i)
-        if (int rc = plan_member(b->eng[i], plans[i], b->spread)) return rc;
-    // Branches in order of decreasing cluster size (then shared memory per CTA):
-    // the GPU places the clusters of the first branches first, and putting the
-    // largest first packs the GPCs best (best-fit decreasing).  On the mixed
-    // L=12/14/16 workload this order measured up to 36 % faster than member
-    // order.
-    std::vector<size_t> order(b->eng.size());
-    for (size_t i = 0; i < order.size(); ++i) order[i] = i;
-    std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) {
-        if (plans[x].K != plans[y].K) return plans[x].K > plans[y].K;
-        return plans[x].smem > plans[y].smem;
-    });
-    CSG_CUDA(cudaStreamBeginCapture(b->main, cudaStreamCaptureModeThreadLocal));
-    int rc = CSG_OK;
-    cudaError_t ce = cudaEventRecord(b->fork, b->main);
-    for (size_t oi = 0; oi < order.size() && rc == CSG_OK && ce == cudaSuccess; ++oi) {
-        const size_t i = order[oi];
-        csg_engine* e = b->eng[i];
-        ce = cudaStreamWaitEvent(e->stream, b->fork, 0);
-        if (ce != cudaSuccess) break;
-        const csg_device_obs o = device_obs(e);
-        rc = run_device(e->cfg, e->spins, e->bonds, with_obs ? &o : nullptr, 0, n_sweeps, e->stream,
-                        0, b->counters + i, &plans[i]);
-        if (rc == CSG_OK) ce = cudaEventRecord(b->join[i], e->stream);
-        if (ce == cudaSuccess) ce = cudaStreamWaitEvent(b->main, b->join[i], 0);
-    }
-    cudaGraph_t g = nullptr;
-    const cudaError_t ce2 = cudaStreamEndCapture(b->main, &g);
-    if (rc != CSG_OK) {
-        if (g) cudaGraphDestroy(g);
-        return rc;
-    }
-    if (ce != cudaSuccess || ce2 != cudaSuccess) {
-        if (g) cudaGraphDestroy(g);
-        return fail(CSG_ERR_CUDA, std::string("graph capture: ") +
-                                      cudaGetErrorString(ce != cudaSuccess ? ce : ce2));
-    }
-    const cudaError_t ce3 = cudaGraphInstantiate(out, g, 0);
-    cudaGraphDestroy(g);
-    if (ce3 != cudaSuccess)
-        return fail(CSG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce3));
-    return CSG_OK;
-}
-
-// Launch the batch graph for n sweeps from the members' host sweep counters.
-int launch_batch(csg_batch* b, int64_t n_sweeps, bool with_obs) {
-    for (csg_engine* e : b->eng) CSG_CUDA(cudaStreamSynchronize(e->stream));
-    cudaGraphExec_t exec = nullptr;
-    if (with_obs)
-        for (auto& g : b->graphs)
-            if (g.first == n_sweeps) exec = g.second;
-    if (!exec) {
-        if (int rc = capture(b, n_sweeps, with_obs, &exec)) return rc;
-        if (with_obs) b->graphs.push_back({n_sweeps, exec});
-    }
-    std::vector<long long> start(b->eng.size());
-    for (size_t i = 0; i < b->eng.size(); ++i) start[i] = b->eng[i]->sweep;
-    CSG_CUDA(cudaMemcpyAsync(b->counters, start.data(), start.size() * sizeof(long long),
-                             cudaMemcpyHostToDevice, b->main));
-    CSG_CUDA(cudaGraphLaunch(exec, b->main));
-    if (!with_obs) {
-        CSG_CUDA(cudaStreamSynchronize(b->main));
-        cudaGraphExecDestroy(exec);
-    }
-    return CSG_OK;
-}
-
-void account(csg_engine* e, int64_t n) {
-    const csg_schedule& sc = e->cfg.sched;
-    e->swap_rounds += count_events(e->sweep, n, sc.sweeps_per_swap, 0);
-    e->n_meas += count_events(e->sweep, n, sc.sweeps_per_meas, sc.meas_start);
-    e->sweep += n;
-}
-
-}  // namespace
-
-extern "C" {
-
-int csg_batch_create(const csg_config* cfgs, int32_t n, csg_batch** out) {
-    if (!out || !cfgs || n < 1) return fail(CSG_ERR_ARG, "bad batch arguments");
-    *out = nullptr;
-    csg_batch* b = new (std::nothrow) csg_batch();
-    if (!b) return fail(CSG_ERR_NOMEM, "host allocation failed");
-    int rc = CSG_OK;
-    for (int i = 0; i < n && rc == CSG_OK; ++i) {
-        csg_engine* e = nullptr;
-        rc = csg_engine_create(&cfgs[i], &e);
-        if (rc == CSG_OK && use_stream(cfgs[i])) {
-            csg_engine_destroy(e);
-            rc = fail(CSG_ERR_UNSUPPORTED,
-                      "batch members need the cluster-resident kernel (L <= 24, no CSG_ENGINE_STREAM)");
-        }
-        if (rc == CSG_OK) b->eng.push_back(e);
-    }
-    if (rc == CSG_OK && cudaStreamCreateWithFlags(&b->main, cudaStreamNonBlocking) != cudaSuccess)
-        rc = fail(CSG_ERR_CUDA, "cudaStreamCreate failed");
-    if (rc == CSG_OK && cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess)
-        rc = fail(CSG_ERR_CUDA, "cudaEventCreate failed");
-    for (int i = 0; i < n && rc == CSG_OK; ++i) {
-        cudaEvent_t ev;
-        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
-            rc = fail(CSG_ERR_CUDA, "cudaEventCreate failed");
-        else
-            b->join.push_back(ev);
-    }
-    if (rc == CSG_OK) rc = dalloc(&b->counters, (size_t)n);
-    if (rc != CSG_OK) {
-        const std::string msg = g_err;
-        csg_batch_destroy(b);
-        g_err = msg;
-        return rc;
-    }
-    *out = b;
-    return CSG_OK;
-}
-
-int csg_batch_destroy(csg_batch* b) {
-    if (!b) return CSG_OK;
-    if (b->main) cudaStreamSynchronize(b->main);
-    drop_graphs(b);
-    for (csg_engine* e : b->eng) csg_engine_destroy(e);
-    for (cudaEvent_t ev : b->join) cudaEventDestroy(ev);
-    if (b->fork) cudaEventDestroy(b->fork);
-    if (b->main) cudaStreamDestroy(b->main);
-    if (b->counters) cudaFree(b->counters);
-    delete b;
-    return CSG_OK;
-}
-
-int csg_batch_engine(csg_batch* b, int32_t i, csg_engine** out) {
-    if (!b || !out || i < 0 || i >= (int32_t)b->eng.size()) return fail(CSG_ERR_ARG, "bad member index");
-    *out = b->eng[i];
-    return CSG_OK;
-}
-
-int csg_batch_run(csg_batch* b, int64_t n_sweeps) {
-    if (!b || n_sweeps < 0) return fail(CSG_ERR_ARG, "bad batch run arguments");
-    if (n_sweeps == 0) return CSG_OK;
-    if (int rc = launch_batch(b, n_sweeps, true)) return rc;
-    CSG_CUDA(cudaStreamSynchronize(b->main));
-    for (csg_engine* e : b->eng) account(e, n_sweeps);
-    return CSG_OK;
-}
-
-int csg_batch_run_sequential(csg_batch* b, int64_t n_sweeps) {
-    if (!b || n_sweeps < 0) return fail(CSG_ERR_ARG, "bad batch run arguments");
-    for (csg_engine* e : b->eng) CSG_CUDA(cudaStreamSynchronize(e->stream));
-    for (csg_engine* e : b->eng) {
-        const csg_device_obs o = device_obs(e);
-        if (int rc = run_device(e->cfg, e->spins, e->bonds, &o, e->sweep, n_sweeps, b->main, e->qc))
-            return rc;
-        account(e, n_sweeps);
-    }
-    CSG_CUDA(cudaStreamSynchronize(b->main));
-    return CSG_OK;
-}
-
-int csg_batch_set_plan(csg_batch* b, const int32_t* quads_per_cta) {
-    if (!b || !quads_per_cta) return fail(CSG_ERR_ARG, "null argument");
-    for (size_t i = 0; i < b->eng.size(); ++i) {
-        const csg_dims& d = b->eng[i]->cfg.dims;
-        const int G = d.n_copies * d.n_temps / 4;
-        if (quads_per_cta[i] < 0 || (quads_per_cta[i] > 0 && G % quads_per_cta[i]))
-            return fail(CSG_ERR_ARG, "quads_per_cta must divide n_copies*n_temps/4");
-    }
-    for (size_t i = 0; i < b->eng.size(); ++i) b->eng[i]->qc = quads_per_cta[i];
-    drop_graphs(b);
-    return CSG_OK;
-}
-
-// Autotuner: times the whole batch graph for probe_sweeps sweeps (best of two)
-// for every combination of the members' quads per CTA, each with and without
-// one SM per CTA, when there are at most 256 such combinations; otherwise
-// coordinate descent over one member at a time
-// with the others fixed (two passes).  The members' spins are saved before and restored
-// after, and the probes accumulate no observables, so tuning leaves the
-// simulations exactly as they were.
-int csg_batch_tune(csg_batch* b, int64_t probe_sweeps, int32_t* chosen) {
-    if (!b || probe_sweeps < 1) return fail(CSG_ERR_ARG, "bad tune arguments");
-    const size_t n = b->eng.size();
-    std::vector<uint32_t*> saved(n, nullptr);
-    int rc = CSG_OK;
-    for (size_t i = 0; i < n && rc == CSG_OK; ++i) {
-        rc = dalloc(&saved[i], b->eng[i]->n_spins);
-        if (rc == CSG_OK)
-            if (cudaMemcpyAsync(saved[i], b->eng[i]->spins, b->eng[i]->n_spins * 4,
-                                cudaMemcpyDeviceToDevice, b->eng[i]->stream) != cudaSuccess)
-                rc = fail(CSG_ERR_CUDA, "snapshot copy failed");
-    }
-    cudaEvent_t t0 = nullptr, t1 = nullptr;
-    if (rc == CSG_OK && (cudaEventCreate(&t0) != cudaSuccess || cudaEventCreate(&t1) != cudaSuccess))
-        rc = fail(CSG_ERR_CUDA, "cudaEventCreate failed");
-    auto time_batch = [&](float& ms_out) -> int {
-        cudaGraphExec_t exec = nullptr;
-        if (int r = capture(b, probe_sweeps, false, &exec)) return r;
-        float best = 1e30f;
-        for (int rep = 0; rep < 3; ++rep) {  // first launch warms up
-            std::vector<long long> start(n, 0);
-            CSG_CUDA(cudaMemcpyAsync(b->counters, start.data(), n * sizeof(long long),
-                                     cudaMemcpyHostToDevice, b->main));
-            CSG_CUDA(cudaEventRecord(t0, b->main));
-            CSG_CUDA(cudaGraphLaunch(exec, b->main));
-            CSG_CUDA(cudaEventRecord(t1, b->main));
-            CSG_CUDA(cudaEventSynchronize(t1));
-            float ms = 0.f;
-            CSG_CUDA(cudaEventElapsedTime(&ms, t0, t1));
-            if (rep > 0 && ms < best) best = ms;
-        }
-        cudaGraphExecDestroy(exec);
-        ms_out = best;
-        return CSG_OK;
-    };
-    for (size_t i = 0; i < n && rc == CSG_OK; ++i) {
-        Plan pl;
-        rc = plan_member(b->eng[i], pl);  // start from the per-member plan
-        if (rc == CSG_OK) b->eng[i]->qc = pl.Qc;
-    }
-    // the quads-per-CTA values each member can take
-    std::vector<std::vector<int>> options(n);
-    size_t combos = 1;
-    for (size_t i = 0; i < n; ++i) {
-        csg_engine* e = b->eng[i];
-        const int G = e->cfg.dims.n_copies * e->cfg.dims.n_temps / 4;
-        const bool gen = e->cfg.H != 0.0;
-        const bool has_m = gen || (e->cfg.flags & CSG_MEASURE_M);
-        for (int qc = 1; qc <= G; ++qc)
-            if (G % qc == 0 && G / qc <= 16 && smem_for(e->cfg.dims.L, qc, has_m, gen) <= kMaxSmem &&
-                qc * csg::tpq_for(e->cfg.dims.L) <= csg::kMaxThreads)
-                options[i].push_back(qc);
-        combos *= std::max<size_t>(1, options[i].size());
-    }
-    if (2 * combos <= 256) {
-        // few enough combinations: time every one, with and without one SM per
-        // CTA (members share the GPU, so the best plan of one member depends
-        // on the others')
-        float best_ms = 1e30f;
-        bool best_spread = false;
-        std::vector<int> best(n);
-        for (size_t i = 0; i < n; ++i) best[i] = b->eng[i]->qc;
-        for (size_t k = 0; k < 2 * combos && rc == CSG_OK; ++k) {
-            b->spread = k >= combos;
-            size_t r = k % combos;
-            for (size_t i = 0; i < n; ++i) {
-                const size_t m = options[i].size();
-                if (m) b->eng[i]->qc = options[i][r % m];
-                r /= std::max<size_t>(1, m);
-            }
-            float ms = 0.f;
-            if (time_batch(ms) != CSG_OK) {  // e.g. a cluster shape the device cannot place
-                cudaGetLastError();
-                continue;
-            }
-            if (ms < best_ms) {
-                best_ms = ms;
-                best_spread = b->spread;
-                for (size_t i = 0; i < n; ++i) best[i] = b->eng[i]->qc;
-            }
-        }
-        for (size_t i = 0; i < n; ++i) b->eng[i]->qc = best[i];
-        b->spread = best_spread;
-    }
-    for (int pass = 0; pass < 2 && rc == CSG_OK && 2 * combos > 256; ++pass)
-        for (size_t i = 0; i < n && rc == CSG_OK; ++i) {
-            csg_engine* e = b->eng[i];
-            int best_qc = e->qc;
-            float best_ms = 1e30f;
-            for (const int qc : options[i]) {
-                e->qc = qc;
-                float ms = 0.f;
-                const int r = time_batch(ms);
-                if (r != CSG_OK) {  // e.g. a cluster shape the device cannot place
-                    cudaGetLastError();
-                    continue;
-                }
-                if (ms < best_ms) {
-                    best_ms = ms;
-                    best_qc = qc;
-                }
-            }
-            e->qc = best_qc;
-        }
-    for (size_t i = 0; i < n; ++i) {
-        if (saved[i]) {
-            if (rc == CSG_OK &&
-                cudaMemcpy(b->eng[i]->spins, saved[i], b->eng[i]->n_spins * 4,
-                           cudaMemcpyDeviceToDevice) != cudaSuccess)
-                rc = fail(CSG_ERR_CUDA, "restore copy failed");
-            cudaFree(saved[i]);
-        }
-        if (chosen) chosen[i] = b->eng[i]->qc;
-    }
-    if (t0) cudaEventDestroy(t0);
-    if (t1) cudaEventDestroy(t1);
-    drop_graphs(b);
-    return rc;
-}
-
-}  // extern "C"
-
-// ---------------------------------------------------------------------------
-// Serving: continuous batching of simulation requests.
-// ---------------------------------------------------------------------------
-namespace {
-
-size_t footprint_bytes(const csg_config& c) {
-    const csg_dims& d = c.dims;
-    const size_t N = (size_t)d.L * d.L * d.L;
-    const size_t ne = (size_t)d.n_words * d.n_copies * d.n_temps * 32;
-    const size_t nq = d.n_copies == 2 ? (size_t)d.n_words * d.n_temps * 32 : 0;
-    const size_t nh = d.n_copies == 2 ? (size_t)d.n_temps * (N + 1) : 0;
-    return (size_t)d.n_words * d.n_copies * d.n_temps * N * 4 + (size_t)d.n_words * 3 * N * 4 +
-           ne * (8 + 8 + 4 + 4) + nq * (8 + 8 + 16 + 4) + nh * 4 +
-           (size_t)d.n_copies * d.n_temps * 8 + (size_t)c.swap_log_rounds * ne / 32 * 4 + 8 +
-           (use_stream(c) ? stream_layout(c).bytes : 0);
-}
-
-// Quads per CTA for a request that shares the GPU with others: the largest
-// split that fits one CTA (fewest CTAs and cluster barriers per unit of work);
-// 0 (the single-request plan) for the streaming engine.
-int shared_gpu_qc(const csg_config& c) {
-    if (use_stream(c)) return 0;
-    const int G = c.dims.n_copies * c.dims.n_temps / 4;
-    const bool gen = !(c.H == 0.0);
-    const bool has_m = gen || (c.flags & CSG_MEASURE_M);
-    int best = 0;
-    for (int qc = 1; qc <= G; ++qc)
-        if (G % qc == 0 && G / qc <= 16 && smem_for(c.dims.L, qc, has_m, gen) <= kMaxSmem &&
-            qc * csg::tpq_for(c.dims.L) <= csg::kMaxThreads)
-            best = qc;
-    return best;
-}
-
-}  // namespace
-
-struct csg_server {
-    struct Req {
-        int64_t id;
-        csg_config cfg;
-        std::vector<double> betas;
-        int64_t total = 0, launched = 0;
-        size_t bytes = 0;
-        csg_engine* e = nullptr;
-        bool done = false;
-    };
-    size_t budget = 0, in_use = 0;
-    int max_active = 0;
-    int64_t chunk = 1024, next_id = 1;
-    std::vector<Req> queue;   // waiting, FIFO
-    std::vector<Req> active;  // admitted (running or finished, result not fetched)
-};
-
-extern "C" {
-
-int csg_engine_footprint(const csg_config* cfg, size_t* bytes) {
-    if (int rc = validate(cfg)) return rc;
-    if (!bytes) return fail(CSG_ERR_ARG, "null output");
-    *bytes = footprint_bytes(*cfg);
-    return CSG_OK;
-}
-
-int csg_server_create(size_t memory_budget_bytes, int32_t max_active, int32_t sweeps_per_launch,
-                      csg_server** out) {
-    if (!out || memory_budget_bytes == 0 || max_active < 1 || sweeps_per_launch < 1)
-        return fail(CSG_ERR_ARG, "bad server arguments");
-    csg_server* s = new (std::nothrow) csg_server();
-    if (!s) return fail(CSG_ERR_NOMEM, "host allocation failed");
-    s->budget = memory_budget_bytes;
-    s->max_active = max_active;
-    s->chunk = sweeps_per_launch;
-    *out = s;
-    return CSG_OK;
-}
-
-int csg_server_destroy(csg_server* s) {
-    if (!s) return CSG_OK;
-    for (auto& r : s->active) csg_engine_destroy(r.e);
-    delete s;
-    return CSG_OK;
-}
-
-int csg_server_submit(csg_server* s, const csg_config* cfg, int64_t n_sweeps, int64_t* id) {
-    if (!s || !id || n_sweeps < 1) return fail(CSG_ERR_ARG, "bad request");
-    if (int rc = validate(cfg)) return rc;
-    csg_server::Req r;
-    r.id = s->next_id++;
-    r.cfg = *cfg;
-    r.betas.assign(cfg->betas, cfg->betas + cfg->dims.n_temps);
-    r.total = n_sweeps;
-    r.bytes = footprint_bytes(*cfg);
-    if (r.bytes > s->budget) return fail(CSG_ERR_NOMEM, "request larger than the memory budget");
-    s->queue.push_back(std::move(r));
-    s->queue.back().cfg.betas = s->queue.back().betas.data();
-    *id = s->queue.back().id;
-    return CSG_OK;
-}
-
-// One non-blocking scheduling pass: completes requests whose device work has
-// drained, admits waiting requests (FIFO, while the budget and the active-slot
-// count allow), and launches the next section of every request whose stream
-// is idle.  Completed ids are reported once.
-int csg_server_poll(csg_server* s, int64_t* completed, int32_t max_completed,
-                    int32_t* n_completed, int32_t* n_active, int32_t* n_queued) {
-    if (!s) return fail(CSG_ERR_ARG, "null server");
-    int32_t nc = 0;
-    for (auto& r : s->active) {
-        if (r.done) continue;
-        const cudaError_t q = cudaStreamQuery(r.e->stream);
-        if (q == cudaErrorNotReady) continue;
-        if (q != cudaSuccess) return fail(CSG_ERR_CUDA, std::string("request stream: ") + cudaGetErrorString(q));
-        if (r.launched >= r.total) {
-            r.done = true;
-            if (completed && nc < max_completed) completed[nc] = r.id;
-            ++nc;
-        }
-    }
-    while (!s->queue.empty() && (int)s->active.size() < s->max_active &&
-           s->in_use + s->queue.front().bytes <= s->budget) {
-        csg_server::Req r = std::move(s->queue.front());
-        s->queue.erase(s->queue.begin());
-        r.cfg.betas = r.betas.data();
-        if (int rc = csg_engine_create(&r.cfg, &r.e)) return rc;
-        if (int rc = csg_init_lattice(r.e)) {
-            csg_engine_destroy(r.e);
-            return rc;
-        }
-        s->in_use += r.bytes;
-        s->active.push_back(std::move(r));
-        s->active.back().cfg.betas = s->active.back().betas.data();
-        s->active.back().e->cfg.betas = s->active.back().e->betas.data();
-    }
-    int running = 0;
-    for (auto& r : s->active) running += (!r.done && r.launched < r.total) ? 1 : 0;
-    for (auto& r : s->active) {
-        if (r.done || r.launched >= r.total) continue;
-        if (cudaStreamQuery(r.e->stream) != cudaSuccess) continue;
-        const int64_t n = std::min<int64_t>(s->chunk, r.total - r.launched);
-        // alone, a request takes the plan that spreads it widest; sharing the
-        // GPU, the one with the fewest CTAs (every plan gives the same bits)
-        r.e->qc = running > 1 ? shared_gpu_qc(r.cfg) : 0;
-        if (int rc = csg_run(r.e, n)) return rc;
-        r.launched += n;
-    }
-    if (n_completed) *n_completed = nc;
-    int32_t na = 0;
-    for (auto& r : s->active) na += r.done ? 0 : 1;
-    if (n_active) *n_active = na;
-    if (n_queued) *n_queued = (int32_t)s->queue.size();
-    return CSG_OK;
-}
-
-// Results of a completed request (observables, optionally the final state in
-// the canonical layout); releases its device memory.
-int csg_server_result(csg_server* s, int64_t id, csg_observables* obs, uint32_t* spins,
-                      size_t n_spins) {
-    if (!s) return fail(CSG_ERR_ARG, "null server");
-    for (size_t i = 0; i < s->active.size(); ++i) {
-        csg_server::Req& r = s->active[i];
-        if (r.id != id) continue;
-        if (!r.done) return fail(CSG_ERR_STATE, "request not completed");
-        int rc = CSG_OK;
-        if (obs) rc = csg_get_observables(r.e, obs);
-        if (rc == CSG_OK && spins) rc = csg_get_state(r.e, spins, n_spins, nullptr, 0, nullptr);
-        if (rc != CSG_OK) return rc;
-        csg_engine_destroy(r.e);
-        s->in_use -= r.bytes;
-        s->active.erase(s->active.begin() + (long)i);
-        return CSG_OK;
-    }
-    return fail(CSG_ERR_ARG, "unknown request id");
-}
-
-}  // extern "C"

@@ -17,10 +17,9 @@
 #include <string>
 
 #include "csg.h"
+#include "engine_internal.h"
 
-namespace csg_detail {
-void set_last_error(const std::string& msg);  // csg_engine.cu (not exported)
-}
+using csg_detail::fail;  // reported by csg_last_error()
 
 namespace {
 
@@ -31,11 +30,6 @@ static __device__ __align__(256) int g_obs_scratch[kScratchInts];
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 int* g_scratch_ptr[kMaxDevices] = {};
-
-int fail(int code, const std::string& msg) {
-    csg_detail::set_last_error(msg);  // reported by csg_last_error()
-    return code;
-}
 
 // The integers of one (word, temperature) pair, lane b = sample 32w+b:
 // bond energy and magnetisation of both copies, number of sites where the

@@ -1,0 +1,160 @@
+// server.cpp — serving: continuous batching of simulation requests.  Requests
+// queue FIFO, are admitted while a device-memory budget and a slot count
+// allow, and run as plain engines on their own streams in sections of a fixed
+// number of sweeps, so that new requests join between sections.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <new>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "csg.h"
+#include "engine_internal.h"
+
+using namespace csg_detail;
+
+namespace {
+
+// Quads per CTA for a request that shares the GPU with others: the largest
+// split that fits one CTA (fewest CTAs and cluster barriers per unit of work);
+// 0 (the single-request plan) for the streaming engine.
+int shared_gpu_qc(const csg_config& c) {
+    const std::vector<int> s = quad_splits(c);
+    return s.empty() ? 0 : s.back();
+}
+
+}  // namespace
+
+struct csg_server {
+    struct Req {
+        int64_t id;
+        csg_config cfg;
+        std::vector<double> betas;
+        int64_t total = 0, launched = 0;
+        size_t bytes = 0;
+        csg_engine* e = nullptr;
+        bool done = false;
+    };
+    size_t budget = 0, in_use = 0;
+    int max_active = 0;
+    int64_t chunk = 1024, next_id = 1;
+    std::vector<Req> queue;   // waiting, FIFO
+    std::vector<Req> active;  // admitted (running or finished, result not fetched)
+};
+
+extern "C" {
+
+int csg_server_create(size_t memory_budget_bytes, int32_t max_active, int32_t sweeps_per_launch,
+                      csg_server** out) {
+    if (!out || memory_budget_bytes == 0 || max_active < 1 || sweeps_per_launch < 1)
+        return fail(CSG_ERR_ARG, "bad server arguments");
+    csg_server* s = new (std::nothrow) csg_server();
+    if (!s) return fail(CSG_ERR_NOMEM, "host allocation failed");
+    s->budget = memory_budget_bytes;
+    s->max_active = max_active;
+    s->chunk = sweeps_per_launch;
+    *out = s;
+    return CSG_OK;
+}
+
+int csg_server_destroy(csg_server* s) {
+    if (!s) return CSG_OK;
+    for (auto& r : s->active) csg_engine_destroy(r.e);
+    delete s;
+    return CSG_OK;
+}
+
+int csg_server_submit(csg_server* s, const csg_config* cfg, int64_t n_sweeps, int64_t* id) {
+    if (!s || !id || n_sweeps < 1) return fail(CSG_ERR_ARG, "bad request");
+    if (int rc = validate(cfg)) return rc;
+    csg_server::Req r;
+    r.id = s->next_id++;
+    r.cfg = *cfg;
+    r.betas.assign(cfg->betas, cfg->betas + cfg->dims.n_temps);
+    r.total = n_sweeps;
+    r.bytes = footprint_bytes(*cfg);
+    if (r.bytes > s->budget) return fail(CSG_ERR_NOMEM, "request larger than the memory budget");
+    s->queue.push_back(std::move(r));
+    s->queue.back().cfg.betas = s->queue.back().betas.data();
+    *id = s->queue.back().id;
+    return CSG_OK;
+}
+
+// One non-blocking scheduling pass: completes requests whose device work has
+// drained, admits waiting requests (FIFO, while the budget and the active-slot
+// count allow), and launches the next section of every request whose stream
+// is idle.  Completed ids are reported once.
+int csg_server_poll(csg_server* s, int64_t* completed, int32_t max_completed,
+                    int32_t* n_completed, int32_t* n_active, int32_t* n_queued) {
+    if (!s) return fail(CSG_ERR_ARG, "null server");
+    int32_t nc = 0;
+    for (auto& r : s->active) {
+        if (r.done) continue;
+        const cudaError_t q = cudaStreamQuery(r.e->stream);
+        if (q == cudaErrorNotReady) continue;
+        if (q != cudaSuccess) return fail(CSG_ERR_CUDA, std::string("request stream: ") + cudaGetErrorString(q));
+        if (r.launched >= r.total) {
+            r.done = true;
+            if (completed && nc < max_completed) completed[nc] = r.id;
+            ++nc;
+        }
+    }
+    while (!s->queue.empty() && (int)s->active.size() < s->max_active &&
+           s->in_use + s->queue.front().bytes <= s->budget) {
+        csg_server::Req r = std::move(s->queue.front());
+        s->queue.erase(s->queue.begin());
+        r.cfg.betas = r.betas.data();
+        if (int rc = csg_engine_create(&r.cfg, &r.e)) return rc;
+        if (int rc = csg_init_lattice(r.e)) {
+            csg_engine_destroy(r.e);
+            return rc;
+        }
+        s->in_use += r.bytes;
+        s->active.push_back(std::move(r));
+        s->active.back().cfg.betas = s->active.back().betas.data();
+        s->active.back().e->cfg.betas = s->active.back().e->betas.data();
+    }
+    int running = 0;
+    for (auto& r : s->active) running += (!r.done && r.launched < r.total) ? 1 : 0;
+    for (auto& r : s->active) {
+        if (r.done || r.launched >= r.total) continue;
+        if (cudaStreamQuery(r.e->stream) != cudaSuccess) continue;
+        const int64_t n = std::min<int64_t>(s->chunk, r.total - r.launched);
+        // alone, a request takes the plan that spreads it widest; sharing the
+        // GPU, the one with the fewest CTAs (every plan gives the same bits)
+        r.e->qc = running > 1 ? shared_gpu_qc(r.cfg) : 0;
+        if (int rc = csg_run(r.e, n)) return rc;
+        r.launched += n;
+    }
+    if (n_completed) *n_completed = nc;
+    int32_t na = 0;
+    for (auto& r : s->active) na += r.done ? 0 : 1;
+    if (n_active) *n_active = na;
+    if (n_queued) *n_queued = (int32_t)s->queue.size();
+    return CSG_OK;
+}
+
+// Results of a completed request (observables, optionally the final state in
+// the canonical layout); releases its device memory.
+int csg_server_result(csg_server* s, int64_t id, csg_observables* obs, uint32_t* spins,
+                      size_t n_spins) {
+    if (!s) return fail(CSG_ERR_ARG, "null server");
+    for (size_t i = 0; i < s->active.size(); ++i) {
+        csg_server::Req& r = s->active[i];
+        if (r.id != id) continue;
+        if (!r.done) return fail(CSG_ERR_STATE, "request not completed");
+        int rc = CSG_OK;
+        if (obs) rc = csg_get_observables(r.e, obs);
+        if (rc == CSG_OK && spins) rc = csg_get_state(r.e, spins, n_spins, nullptr, 0, nullptr);
+        if (rc != CSG_OK) return rc;
+        csg_engine_destroy(r.e);
+        s->in_use -= r.bytes;
+        s->active.erase(s->active.begin() + (long)i);
+        return CSG_OK;
+    }
+    return fail(CSG_ERR_ARG, "unknown request id");
+}
+
+}  // extern "C"
