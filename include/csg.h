@@ -289,7 +289,10 @@ int csg_server_poll(csg_server* s, int64_t* completed, int32_t max_completed,
                     int32_t* n_completed, int32_t* n_active, int32_t* n_queued);
 
 /* Observables (and optionally the final spins) of a completed request;
- * releases its memory.  Any output pointer may be NULL. */
+ * releases its memory.  Any output pointer may be NULL.  A request whose
+ * engine could not be created at admission (e.g. device memory exhausted) or
+ * whose launch failed is reported completed by csg_server_poll; this call
+ * then returns that error code (message in csg_last_error) and releases it. */
 int csg_server_result(csg_server* s, int64_t id, csg_observables* obs, uint32_t* spins,
                       size_t n_spins);
 

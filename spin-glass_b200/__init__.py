@@ -425,6 +425,9 @@ class Server:
         return [int(i) for i in ids[:min(nc.value, max_completed)]], na.value, nq.value
 
     def result(self, rid: int, with_spins: bool = False):
+        if rid not in self._req:  # the library reports the unknown id
+            _check(lib().csg_server_result(self._h, rid, None, None, 0))
+            return None
         L, W, C_, T = self._req.pop(rid)
         o = Observables(L, W, C_, T)
         spins = np.zeros((W, C_, T // 4, L ** 3, 4), np.uint32) if with_spins else None

@@ -634,8 +634,9 @@ int csg_engine_create(const csg_config* cfg, csg_engine** out) {
     e->n_q = d.n_copies == 2 ? (size_t)d.n_words * d.n_temps * 32 : 0;
     e->n_hist = d.n_copies == 2 ? (size_t)d.n_temps * (N + 1) : 0;
     int rc = CSG_OK;
-    auto chk = [&](int r) {
-        if (rc == CSG_OK) rc = r;
+    // stops at the first failure (nothing more is allocated)
+    auto alloc = [&](auto** p, size_t n) {
+        if (rc == CSG_OK) rc = dalloc(p, n);
     };
     if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
         cudaGetLastError();
@@ -643,20 +644,20 @@ int csg_engine_create(const csg_config* cfg, csg_engine** out) {
         delete e;
         return fail(CSG_ERR_CUDA, "cudaStreamCreate failed");
     }
-    chk(dalloc(&e->spins, e->n_spins));
-    chk(dalloc(&e->bonds, e->n_bonds));
-    chk(dalloc(&e->e_sum, e->n_e));
-    chk(dalloc(&e->m_sum, e->n_e));
-    chk(dalloc(&e->e_last, e->n_e));
-    chk(dalloc(&e->m_last, e->n_e));
-    chk(dalloc(&e->q_sum, e->n_q));
-    chk(dalloc(&e->q2_sum, e->n_q));
-    chk(dalloc(&e->q4_sum, 2 * e->n_q));
-    chk(dalloc(&e->d_last, e->n_q));
-    chk(dalloc(&e->hist, e->n_hist));
-    chk(dalloc(&e->swap_acc, (size_t)d.n_copies * d.n_temps));
-    chk(dalloc(&e->swap_log, (size_t)cfg->swap_log_rounds * e->n_e / 32));
-    chk(dalloc(&e->boundary, 1));
+    alloc(&e->spins, e->n_spins);
+    alloc(&e->bonds, e->n_bonds);
+    alloc(&e->e_sum, e->n_e);
+    alloc(&e->m_sum, e->n_e);
+    alloc(&e->e_last, e->n_e);
+    alloc(&e->m_last, e->n_e);
+    alloc(&e->q_sum, e->n_q);
+    alloc(&e->q2_sum, e->n_q);
+    alloc(&e->q4_sum, 2 * e->n_q);
+    alloc(&e->d_last, e->n_q);
+    alloc(&e->hist, e->n_hist);
+    alloc(&e->swap_acc, (size_t)d.n_copies * d.n_temps);
+    alloc(&e->swap_log, (size_t)cfg->swap_log_rounds * e->n_e / 32);
+    alloc(&e->boundary, 1);
     if (rc == CSG_OK) rc = reset_obs(e);
     if (rc == CSG_OK) {
         // A launch plan must exist before the engine is handed out.

@@ -36,6 +36,10 @@ struct csg_server {
         size_t bytes = 0;
         csg_engine* e = nullptr;
         bool done = false;
+        // a request whose engine could not be created or launched completes
+        // with this error, which csg_server_result returns
+        int status = CSG_OK;
+        std::string error;
     };
     size_t budget = 0, in_use = 0;
     int max_active = 0;
@@ -61,7 +65,8 @@ int csg_server_create(size_t memory_budget_bytes, int32_t max_active, int32_t sw
 
 int csg_server_destroy(csg_server* s) {
     if (!s) return CSG_OK;
-    for (auto& r : s->active) csg_engine_destroy(r.e);
+    for (auto& r : s->active)
+        if (r.e) csg_engine_destroy(r.e);
     delete s;
     return CSG_OK;
 }
@@ -90,31 +95,41 @@ int csg_server_poll(csg_server* s, int64_t* completed, int32_t max_completed,
                     int32_t* n_completed, int32_t* n_active, int32_t* n_queued) {
     if (!s) return fail(CSG_ERR_ARG, "null server");
     int32_t nc = 0;
+    auto report = [&](csg_server::Req& r) {
+        r.done = true;
+        if (completed && nc < max_completed) completed[nc] = r.id;
+        ++nc;
+    };
+    // a failed request gives its memory back at once; its id is reported done
+    auto failed = [&](csg_server::Req& r, int rc) {
+        r.status = rc;
+        r.error = last_error();
+        if (r.e) {
+            csg_engine_destroy(r.e);
+            r.e = nullptr;
+            s->in_use -= r.bytes;
+        }
+        report(r);
+    };
     for (auto& r : s->active) {
         if (r.done) continue;
         const cudaError_t q = cudaStreamQuery(r.e->stream);
         if (q == cudaErrorNotReady) continue;
         if (q != cudaSuccess) return fail(CSG_ERR_CUDA, std::string("request stream: ") + cudaGetErrorString(q));
-        if (r.launched >= r.total) {
-            r.done = true;
-            if (completed && nc < max_completed) completed[nc] = r.id;
-            ++nc;
-        }
+        if (r.launched >= r.total) report(r);
     }
     while (!s->queue.empty() && (int)s->active.size() < s->max_active &&
            s->in_use + s->queue.front().bytes <= s->budget) {
-        csg_server::Req r = std::move(s->queue.front());
+        s->active.push_back(std::move(s->queue.front()));
         s->queue.erase(s->queue.begin());
+        csg_server::Req& r = s->active.back();
         r.cfg.betas = r.betas.data();
-        if (int rc = csg_engine_create(&r.cfg, &r.e)) return rc;
-        if (int rc = csg_init_lattice(r.e)) {
-            csg_engine_destroy(r.e);
-            return rc;
+        int rc = csg_engine_create(&r.cfg, &r.e);
+        if (rc == CSG_OK) {
+            s->in_use += r.bytes;
+            rc = csg_init_lattice(r.e);
         }
-        s->in_use += r.bytes;
-        s->active.push_back(std::move(r));
-        s->active.back().cfg.betas = s->active.back().betas.data();
-        s->active.back().e->cfg.betas = s->active.back().e->betas.data();
+        if (rc != CSG_OK) failed(r, rc);
     }
     int running = 0;
     for (auto& r : s->active) running += (!r.done && r.launched < r.total) ? 1 : 0;
@@ -125,7 +140,10 @@ int csg_server_poll(csg_server* s, int64_t* completed, int32_t max_completed,
         // alone, a request takes the plan that spreads it widest; sharing the
         // GPU, the one with the fewest CTAs (every plan gives the same bits)
         r.e->qc = running > 1 ? shared_gpu_qc(r.cfg) : 0;
-        if (int rc = csg_run(r.e, n)) return rc;
+        if (int rc = csg_run(r.e, n)) {
+            failed(r, rc);
+            continue;
+        }
         r.launched += n;
     }
     if (n_completed) *n_completed = nc;
@@ -145,6 +163,12 @@ int csg_server_result(csg_server* s, int64_t id, csg_observables* obs, uint32_t*
         csg_server::Req& r = s->active[i];
         if (r.id != id) continue;
         if (!r.done) return fail(CSG_ERR_STATE, "request not completed");
+        if (r.status != CSG_OK) {
+            const int st = r.status;
+            const std::string msg = "request " + std::to_string(id) + ": " + r.error;
+            s->active.erase(s->active.begin() + (long)i);
+            return fail(st, msg);
+        }
         int rc = CSG_OK;
         if (obs) rc = csg_get_observables(r.e, obs);
         if (rc == CSG_OK && spins) rc = csg_get_state(r.e, spins, n_spins, nullptr, 0, nullptr);

@@ -69,3 +69,54 @@ def test_mixed_requests_equal_alone(csg):
         np.testing.assert_array_equal(o_srv.e_sum, o.e_sum)
         np.testing.assert_array_equal(o_srv.q2_sum, o.q2_sum)
         assert o_srv.n_meas == o.n_meas
+
+
+@pytest.mark.gpu
+def test_request_that_cannot_be_allocated_completes_with_an_error(csg):
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    small, n = request(0)
+    # L=128, 8192 samples, 2 copies, 64 temperatures: 275 GB of spins, more
+    # than the device holds, inside a 1 TiB budget
+    huge = dict(L=128, n_words=256, n_copies=2, betas=np.linspace(0.5, 2.0, 64), seed=7)
+    assert csg.footprint(**huge) > 200e9
+    with csg.Server(1 << 40, max_active=4, sweeps_per_launch=16) as srv:
+        a = srv.submit(n, **small)
+        b = srv.submit(10, **huge)
+        c = srv.submit(n, **dict(small, seed=2000))
+        done, deadline = set(), time.time() + 60
+        while len(done) < 3 and time.time() < deadline:
+            done.update(srv.poll()[0])
+            time.sleep(0.001)
+        assert done == {a, b, c}
+        with pytest.raises(csg.CsgError, match="cudaMalloc"):
+            srv.result(b)
+        o_a, o_c = srv.result(a), srv.result(c)
+        assert srv.poll()[1:] == (0, 0)
+    with csg.Engine(**small) as e:
+        e.init_lattice()
+        e.run(n)
+        o = e.observables()
+    np.testing.assert_array_equal(o_a.e_sum, o.e_sum)
+    assert o_c.n_meas == o.n_meas
+
+
+def test_request_without_a_device_completes_with_an_error(csg):
+    """Host-side failure path: with no CUDA device the engine of an admitted
+    request cannot be created; the request is reported completed and its
+    result call raises the creation error (no GPU involved)."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("needs a host without a CUDA device")
+    kw, n = request(0)
+    with csg.Server(1 << 30, max_active=2, sweeps_per_launch=16) as srv:
+        a = srv.submit(n, **kw)
+        b = srv.submit(n, **dict(kw, seed=5))
+        done, na, nq = srv.poll()
+        assert sorted(done) == [a, b] and (na, nq) == (0, 0)
+        for r in (a, b):
+            with pytest.raises(csg.CsgError, match=f"request {r}"):
+                srv.result(r)
+        with pytest.raises(csg.CsgError, match="unknown request"):
+            srv.result(a)
