@@ -11,7 +11,9 @@ import pytest
 
 ROOT = pathlib.Path(__file__).resolve().parents[1]
 CLI = ROOT / "spin-glass_b200" / "csg"
-REFERENCE = pathlib.Path("/root/reference")
+# The reference checkout: $CSG_REFERENCE_ROOT, else a directory "reference"
+# beside this repository (tests that need it skip when it is absent).
+REFERENCE = pathlib.Path(os.environ.get("CSG_REFERENCE_ROOT", str(ROOT.parent / "reference")))
 
 
 def run_cli(args, cwd):
