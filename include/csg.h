@@ -199,8 +199,10 @@ int csg_init_device(const csg_config* cfg, uint32_t* spins, uint32_t* bonds, voi
  * reference, whose launch shape is fixed at eamsim.cu:695). */
 int csg_query_plan(const csg_config* cfg, csg_plan* out);
 
-/* Force quads_per_cta for later launches (must divide n_copies*n_temps/4);
- * NULL or quads_per_cta == 0 restores the automatic plan. */
+/* Force quads_per_cta (must divide n_copies*n_temps/4) and/or
+ * threads_per_quad (L * L/2 * s for a built column split s) for later launches
+ * of the resident kernel; a zero field keeps that part automatic, NULL
+ * restores the automatic plan. */
 int csg_set_plan_override(const csg_plan* plan);
 
 /* No counterpart in the reference.  The observable records of
@@ -252,17 +254,32 @@ int csg_batch_engine(csg_batch* b, int32_t i, csg_engine** out);
  * first use for this n_sweeps and replayed afterwards). */
 int csg_batch_run(csg_batch* b, int64_t n_sweeps);
 
-/* The same work as the plain engine would do it: member after member. */
+/* The same work as the plain engine would do it: member after member, each
+ * with the plan it would take alone. */
 int csg_batch_run_sequential(csg_batch* b, int64_t n_sweeps);
 
-/* Autotuner: chooses each member's quads per CTA (hence its cluster size), and
- * whether every member CTA gets an SM of its own, by timing the whole batch
- * for probe_sweeps sweeps; states are restored after.  chosen (may be NULL)
- * receives the quads per CTA per member. */
+/* Queue n_sweeps sweeps of every member on `stream` (a cudaStream_t; NULL =
+ * legacy default stream) without waiting: plain == 0 launches the batch graph
+ * (as csg_batch_run), plain == 1 the plain engine member after member (as
+ * csg_batch_run_sequential).  The launch is ordered after the work already
+ * queued on the members' streams and before work queued on them later (state
+ * and observable calls on a member wait for it).  For timing on the caller's
+ * stream. */
+int csg_batch_launch(csg_batch* b, int64_t n_sweeps, int32_t plain, void* stream);
+
+/* Autotuner: chooses each member's tile — quads per CTA (hence its cluster
+ * size) and threads per quad (how many z-segments a column of the checkerboard
+ * is split into) — and whether every member CTA gets an SM of its own, by
+ * timing the whole batch graph for probe_sweeps sweeps; states are restored
+ * after.  chosen (may be NULL) receives the quads per CTA per member;
+ * csg_batch_member_plan reports the whole plan. */
 int csg_batch_tune(csg_batch* b, int64_t probe_sweeps, int32_t* chosen);
 
-/* Set each member's quads per CTA (0 = automatic). */
+/* Set each member's quads per CTA (0 = automatic; threads per quad automatic). */
 int csg_batch_set_plan(csg_batch* b, const int32_t* quads_per_cta);
+
+/* The launch plan member i runs with (after csg_batch_tune: the tuned one). */
+int csg_batch_member_plan(csg_batch* b, int32_t i, csg_plan* out);
 
 /* ---- Serving: continuous batching -------------------------------------------
  * No counterpart in the reference.  Requests (full simulation configurations

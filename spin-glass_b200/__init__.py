@@ -105,6 +105,8 @@ def lib():
             "csg_batch_run_sequential": [vp, i64],
             "csg_batch_tune": [vp, i64, vp],
             "csg_batch_set_plan": [vp, vp],
+            "csg_batch_member_plan": [vp, C.c_int32, C.POINTER(Plan)],
+            "csg_batch_launch": [vp, i64, C.c_int32, vp],
             "csg_engine_footprint": [C.POINTER(Config), C.POINTER(sz)],
             "csg_server_create": [sz, C.c_int32, C.c_int32, C.POINTER(vp)],
             "csg_server_destroy": [vp],
@@ -268,11 +270,13 @@ def query_plan(L: int, n_words: int, n_copies: int, betas, **kw) -> Plan:
     return p
 
 
-def set_plan_override(quads_per_cta: int | None) -> None:
-    if quads_per_cta is None:
+def set_plan_override(quads_per_cta: int | None, threads_per_quad: int = 0) -> None:
+    """Force quads per CTA and/or threads per quad (0: automatic) of later
+    resident-kernel launches; None restores the automatic plan."""
+    if quads_per_cta is None and not threads_per_quad:
         _check(lib().csg_set_plan_override(None))
     else:
-        p = Plan(quads_per_cta, 0, 0, 0)
+        p = Plan(quads_per_cta or 0, 0, threads_per_quad, 0)
         _check(lib().csg_set_plan_override(C.byref(p)))
 
 
@@ -364,6 +368,11 @@ class Batch:
     def run_sequential(self, n_sweeps: int) -> None:
         _check(lib().csg_batch_run_sequential(self._h, n_sweeps))
 
+    def launch(self, n_sweeps: int, stream: int = 0, plain: bool = False) -> None:
+        """Queue n_sweeps sweeps of every member on a CUDA stream (handle as an
+        int, e.g. torch.cuda.current_stream().cuda_stream) without waiting."""
+        _check(lib().csg_batch_launch(self._h, n_sweeps, 1 if plain else 0, C.c_void_p(stream)))
+
     def tune(self, probe_sweeps: int = 64):
         out = np.zeros(len(self.members), np.int32)
         _check(lib().csg_batch_tune(self._h, probe_sweeps, _p(out)))
@@ -372,6 +381,12 @@ class Batch:
     def set_plan(self, quads_per_cta) -> None:
         q = np.ascontiguousarray(quads_per_cta, np.int32)
         _check(lib().csg_batch_set_plan(self._h, _p(q)))
+
+    def member_plan(self, i: int) -> "Plan":
+        """Launch plan member i runs with (the tuned one after tune())."""
+        out = Plan()
+        _check(lib().csg_batch_member_plan(self._h, i, C.byref(out)))
+        return out
 
 
 def footprint(L: int, n_words: int, n_copies: int, betas, **kw) -> int:

@@ -21,6 +21,9 @@ struct csg_batch {
     cudaStream_t main = nullptr;
     cudaEvent_t fork = nullptr;
     std::vector<cudaEvent_t> join;
+    // ordering of launches on a caller's stream against the members' streams
+    std::vector<cudaEvent_t> ready;
+    cudaEvent_t done = nullptr;
     long long* counters = nullptr;  // device sweep counter per member
     std::vector<std::pair<int64_t, cudaGraphExec_t>> graphs;
     // pad every member CTA's shared memory past half an SM, so that no two
@@ -63,7 +66,7 @@ int capture(csg_batch* b, int64_t n_sweeps, bool with_obs, cudaGraphExec_t* out)
         if (ce != cudaSuccess) break;
         const csg_device_obs o = device_obs(e);
         rc = run_device(e->cfg, e->spins, e->bonds, with_obs ? &o : nullptr, 0, n_sweeps, e->stream,
-                        0, b->counters + i, &plans[i]);
+                        PlanChoice{}, b->counters + i, &plans[i]);
         if (rc == CSG_OK) ce = cudaEventRecord(b->join[i], e->stream);
         if (ce == cudaSuccess) ce = cudaStreamWaitEvent(b->main, b->join[i], 0);
     }
@@ -85,26 +88,40 @@ int capture(csg_batch* b, int64_t n_sweeps, bool with_obs, cudaGraphExec_t* out)
     return CSG_OK;
 }
 
-// Launch the batch graph for n sweeps from the members' host sweep counters.
-int launch_batch(csg_batch* b, int64_t n_sweeps, bool with_obs) {
-    for (csg_engine* e : b->eng) CSG_CUDA(cudaStreamSynchronize(e->stream));
-    cudaGraphExec_t exec = nullptr;
-    if (with_obs)
+// Queue n sweeps of every member on stream st: after the work already queued
+// on the members' own streams, and before anything queued on them later.
+// plain = false: one launch of the batch graph (captured on first use for this
+// n_sweeps and replayed afterwards) from the members' host sweep counters;
+// plain = true: the plain engine, member after member, each with its own
+// automatic plan.  The members' host counters advance at once.
+int launch_batch(csg_batch* b, int64_t n_sweeps, bool plain, cudaStream_t st) {
+    for (size_t i = 0; i < b->eng.size(); ++i) {
+        CSG_CUDA(cudaEventRecord(b->ready[i], b->eng[i]->stream));
+        CSG_CUDA(cudaStreamWaitEvent(st, b->ready[i], 0));
+    }
+    if (plain) {
+        for (csg_engine* e : b->eng) {
+            const csg_device_obs o = device_obs(e);
+            if (int rc = run_device(e->cfg, e->spins, e->bonds, &o, e->sweep, n_sweeps, st)) return rc;
+        }
+    } else {
+        cudaGraphExec_t exec = nullptr;
         for (auto& g : b->graphs)
             if (g.first == n_sweeps) exec = g.second;
-    if (!exec) {
-        if (int rc = capture(b, n_sweeps, with_obs, &exec)) return rc;
-        if (with_obs) b->graphs.push_back({n_sweeps, exec});
+        if (!exec) {
+            if (int rc = capture(b, n_sweeps, true, &exec)) return rc;
+            b->graphs.push_back({n_sweeps, exec});
+        }
+        std::vector<long long> start(b->eng.size());
+        for (size_t i = 0; i < b->eng.size(); ++i) start[i] = b->eng[i]->sweep;
+        // pageable source: staged before the call returns
+        CSG_CUDA(cudaMemcpyAsync(b->counters, start.data(), start.size() * sizeof(long long),
+                                 cudaMemcpyHostToDevice, st));
+        CSG_CUDA(cudaGraphLaunch(exec, st));
     }
-    std::vector<long long> start(b->eng.size());
-    for (size_t i = 0; i < b->eng.size(); ++i) start[i] = b->eng[i]->sweep;
-    CSG_CUDA(cudaMemcpyAsync(b->counters, start.data(), start.size() * sizeof(long long),
-                             cudaMemcpyHostToDevice, b->main));
-    CSG_CUDA(cudaGraphLaunch(exec, b->main));
-    if (!with_obs) {
-        CSG_CUDA(cudaStreamSynchronize(b->main));
-        cudaGraphExecDestroy(exec);
-    }
+    CSG_CUDA(cudaEventRecord(b->done, st));
+    for (csg_engine* e : b->eng) CSG_CUDA(cudaStreamWaitEvent(e->stream, b->done, 0));
+    for (csg_engine* e : b->eng) account(e, n_sweeps);
     return CSG_OK;
 }
 
@@ -133,12 +150,20 @@ int csg_batch_create(const csg_config* cfgs, int32_t n, csg_batch** out) {
     if (rc == CSG_OK && cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess)
         rc = fail(CSG_ERR_CUDA, "cudaEventCreate failed");
     for (int i = 0; i < n && rc == CSG_OK; ++i) {
-        cudaEvent_t ev;
+        cudaEvent_t ev, ev2;
         if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
             rc = fail(CSG_ERR_CUDA, "cudaEventCreate failed");
         else
             b->join.push_back(ev);
+        if (rc == CSG_OK) {
+            if (cudaEventCreateWithFlags(&ev2, cudaEventDisableTiming) != cudaSuccess)
+                rc = fail(CSG_ERR_CUDA, "cudaEventCreate failed");
+            else
+                b->ready.push_back(ev2);
+        }
     }
+    if (rc == CSG_OK && cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) != cudaSuccess)
+        rc = fail(CSG_ERR_CUDA, "cudaEventCreate failed");
     if (rc == CSG_OK) rc = dalloc(&b->counters, (size_t)n);
     if (rc != CSG_OK) {
         const std::string msg = last_error();
@@ -155,7 +180,11 @@ int csg_batch_destroy(csg_batch* b) {
     if (b->main) cudaStreamSynchronize(b->main);
     drop_graphs(b);
     for (csg_engine* e : b->eng) csg_engine_destroy(e);
+    for (csg_engine* e : b->eng)
+        if (e->stream) cudaStreamSynchronize(e->stream);
     for (cudaEvent_t ev : b->join) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : b->ready) cudaEventDestroy(ev);
+    if (b->done) cudaEventDestroy(b->done);
     if (b->fork) cudaEventDestroy(b->fork);
     if (b->main) cudaStreamDestroy(b->main);
     if (b->counters) cudaFree(b->counters);
@@ -172,23 +201,24 @@ int csg_batch_engine(csg_batch* b, int32_t i, csg_engine** out) {
 int csg_batch_run(csg_batch* b, int64_t n_sweeps) {
     if (!b || n_sweeps < 0) return fail(CSG_ERR_ARG, "bad batch run arguments");
     if (n_sweeps == 0) return CSG_OK;
-    if (int rc = launch_batch(b, n_sweeps, true)) return rc;
+    if (int rc = launch_batch(b, n_sweeps, false, b->main)) return rc;
     CSG_CUDA(cudaStreamSynchronize(b->main));
-    for (csg_engine* e : b->eng) account(e, n_sweeps);
     return CSG_OK;
 }
 
 int csg_batch_run_sequential(csg_batch* b, int64_t n_sweeps) {
     if (!b || n_sweeps < 0) return fail(CSG_ERR_ARG, "bad batch run arguments");
-    for (csg_engine* e : b->eng) CSG_CUDA(cudaStreamSynchronize(e->stream));
-    for (csg_engine* e : b->eng) {
-        const csg_device_obs o = device_obs(e);
-        if (int rc = run_device(e->cfg, e->spins, e->bonds, &o, e->sweep, n_sweeps, b->main, e->qc))
-            return rc;
-        account(e, n_sweeps);
-    }
+    if (n_sweeps == 0) return CSG_OK;
+    if (int rc = launch_batch(b, n_sweeps, true, b->main)) return rc;
     CSG_CUDA(cudaStreamSynchronize(b->main));
     return CSG_OK;
+}
+
+int csg_batch_launch(csg_batch* b, int64_t n_sweeps, int32_t plain, void* stream) {
+    if (!b || n_sweeps < 0 || (plain != 0 && plain != 1))
+        return fail(CSG_ERR_ARG, "bad batch launch arguments");
+    if (n_sweeps == 0) return CSG_OK;
+    return launch_batch(b, n_sweeps, plain != 0, (cudaStream_t)stream);
 }
 
 int csg_batch_set_plan(csg_batch* b, const int32_t* quads_per_cta) {
@@ -199,8 +229,22 @@ int csg_batch_set_plan(csg_batch* b, const int32_t* quads_per_cta) {
         if (quads_per_cta[i] < 0 || (quads_per_cta[i] > 0 && G % quads_per_cta[i]))
             return fail(CSG_ERR_ARG, "quads_per_cta must divide n_copies*n_temps/4");
     }
-    for (size_t i = 0; i < b->eng.size(); ++i) b->eng[i]->qc = quads_per_cta[i];
+    for (size_t i = 0; i < b->eng.size(); ++i) {
+        b->eng[i]->qc = quads_per_cta[i];
+        b->eng[i]->nseg = 0;
+    }
     drop_graphs(b);
+    return CSG_OK;
+}
+
+int csg_batch_member_plan(csg_batch* b, int32_t i, csg_plan* out) {
+    if (!b || !out || i < 0 || i >= (int32_t)b->eng.size()) return fail(CSG_ERR_ARG, "bad member index");
+    Plan pl;
+    if (int rc = plan_engine(b->eng[i], pl, b->spread ? kSpreadSmem : 0)) return rc;
+    out->quads_per_cta = pl.Qc;
+    out->ctas_per_word = pl.K;
+    out->threads_per_quad = pl.TPQ;
+    out->smem_bytes = (int32_t)pl.smem;
     return CSG_OK;
 }
 
@@ -223,6 +267,10 @@ int csg_batch_tune(csg_batch* b, int64_t probe_sweeps, int32_t* chosen) {
                                 cudaMemcpyDeviceToDevice, b->eng[i]->stream) != cudaSuccess)
                 rc = fail(CSG_ERR_CUDA, "snapshot copy failed");
     }
+    // the probes run on the batch's own stream: the snapshots must be complete
+    for (size_t i = 0; i < n && rc == CSG_OK; ++i)
+        if (cudaStreamSynchronize(b->eng[i]->stream) != cudaSuccess)
+            rc = fail(CSG_ERR_CUDA, "snapshot copy failed");
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     if (rc == CSG_OK && (cudaEventCreate(&t0) != cudaSuccess || cudaEventCreate(&t1) != cudaSuccess))
         rc = fail(CSG_ERR_CUDA, "cudaEventCreate failed");
@@ -249,29 +297,37 @@ int csg_batch_tune(csg_batch* b, int64_t probe_sweeps, int32_t* chosen) {
     for (size_t i = 0; i < n && rc == CSG_OK; ++i) {
         Plan pl;
         rc = plan_engine(b->eng[i], pl);  // start from the per-member plan
-        if (rc == CSG_OK) b->eng[i]->qc = pl.Qc;
+        if (rc == CSG_OK) {
+            b->eng[i]->qc = pl.Qc;
+            b->eng[i]->nseg = pl.NSEG;
+        }
     }
-    // the quads-per-CTA values each member can take
-    std::vector<std::vector<int>> options(n);
+    // the (quads per CTA, column segments per thread) plans each member can take
+    std::vector<std::vector<PlanChoice>> options(n);
     size_t combos = 1;
     for (size_t i = 0; i < n; ++i) {
-        options[i] = quad_splits(b->eng[i]->cfg);
+        options[i] = plan_options(b->eng[i]->cfg);
         combos *= std::max<size_t>(1, options[i].size());
     }
+    auto set_choice = [&](size_t i, const PlanChoice& pc) {
+        b->eng[i]->qc = pc.qc;
+        b->eng[i]->nseg = pc.nseg;
+    };
+    auto choice_of = [&](size_t i) { return PlanChoice{b->eng[i]->qc, b->eng[i]->nseg}; };
     if (2 * combos <= 256) {
         // few enough combinations: time every one, with and without one SM per
         // CTA (members share the GPU, so the best plan of one member depends
         // on the others')
         float best_ms = 1e30f;
         bool best_spread = false;
-        std::vector<int> best(n);
-        for (size_t i = 0; i < n; ++i) best[i] = b->eng[i]->qc;
+        std::vector<PlanChoice> best(n);
+        for (size_t i = 0; i < n; ++i) best[i] = choice_of(i);
         for (size_t k = 0; k < 2 * combos && rc == CSG_OK; ++k) {
             b->spread = k >= combos;
             size_t r = k % combos;
             for (size_t i = 0; i < n; ++i) {
                 const size_t m = options[i].size();
-                if (m) b->eng[i]->qc = options[i][r % m];
+                if (m) set_choice(i, options[i][r % m]);
                 r /= std::max<size_t>(1, m);
             }
             float ms = 0.f;
@@ -282,19 +338,18 @@ int csg_batch_tune(csg_batch* b, int64_t probe_sweeps, int32_t* chosen) {
             if (ms < best_ms) {
                 best_ms = ms;
                 best_spread = b->spread;
-                for (size_t i = 0; i < n; ++i) best[i] = b->eng[i]->qc;
+                for (size_t i = 0; i < n; ++i) best[i] = choice_of(i);
             }
         }
-        for (size_t i = 0; i < n; ++i) b->eng[i]->qc = best[i];
+        for (size_t i = 0; i < n; ++i) set_choice(i, best[i]);
         b->spread = best_spread;
     }
     for (int pass = 0; pass < 2 && rc == CSG_OK && 2 * combos > 256; ++pass)
         for (size_t i = 0; i < n && rc == CSG_OK; ++i) {
-            csg_engine* e = b->eng[i];
-            int best_qc = e->qc;
+            PlanChoice best_pc = choice_of(i);
             float best_ms = 1e30f;
-            for (const int qc : options[i]) {
-                e->qc = qc;
+            for (const PlanChoice& pc : options[i]) {
+                set_choice(i, pc);
                 float ms = 0.f;
                 const int r = time_batch(ms);
                 if (r != CSG_OK) {  // e.g. a cluster shape the device cannot place
@@ -303,10 +358,10 @@ int csg_batch_tune(csg_batch* b, int64_t probe_sweeps, int32_t* chosen) {
                 }
                 if (ms < best_ms) {
                     best_ms = ms;
-                    best_qc = qc;
+                    best_pc = pc;
                 }
             }
-            e->qc = best_qc;
+            set_choice(i, best_pc);
         }
     for (size_t i = 0; i < n; ++i) {
         if (saved[i]) {

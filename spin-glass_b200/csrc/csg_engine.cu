@@ -20,6 +20,11 @@
 #include "aux_kernels.cuh"
 #include "stream_kernels.cuh"
 
+namespace csg {
+// Advances a device-resident sweep counter after a launch of a captured graph.
+__global__ void advance_counter(long long* counter, long long n) { *counter += n; }
+}  // namespace csg
+
 namespace csg_detail {
 
 namespace {
@@ -115,26 +120,23 @@ bool build_tables(const csg_config& cfg, csg::PtTables& tab) {
     return h0_exact && cfg.H == 0.0;
 }
 
-using KernelFn = void (*)(csg::PtParams);
+using KernelFn = csg::ResidentFn;
 
-template <int L>
-KernelFn kernel_for(bool gen) {
-    return gen ? csg::pt_resident_kernel<L, true> : csg::pt_resident_kernel<L, false>;
-}
-
-KernelFn select_kernel(int L, bool gen) {
+// The resident kernel for L (general-field variant when gen) with nseg column
+// segments per thread; nullptr if that variant is not built.
+KernelFn select_kernel(int L, bool gen, int nseg) {
     switch (L) {
-        case 4: return kernel_for<4>(gen);
-        case 6: return kernel_for<6>(gen);
-        case 8: return kernel_for<8>(gen);
-        case 10: return kernel_for<10>(gen);
-        case 12: return kernel_for<12>(gen);
-        case 14: return kernel_for<14>(gen);
-        case 16: return kernel_for<16>(gen);
-        case 18: return kernel_for<18>(gen);
-        case 20: return kernel_for<20>(gen);
-        case 22: return kernel_for<22>(gen);
-        case 24: return kernel_for<24>(gen);
+        case 4: return csg::resident_kernel_L4(gen, nseg);
+        case 6: return csg::resident_kernel_L6(gen, nseg);
+        case 8: return csg::resident_kernel_L8(gen, nseg);
+        case 10: return csg::resident_kernel_L10(gen, nseg);
+        case 12: return csg::resident_kernel_L12(gen, nseg);
+        case 14: return csg::resident_kernel_L14(gen, nseg);
+        case 16: return csg::resident_kernel_L16(gen, nseg);
+        case 18: return csg::resident_kernel_L18(gen, nseg);
+        case 20: return csg::resident_kernel_L20(gen, nseg);
+        case 22: return csg::resident_kernel_L22(gen, nseg);
+        case 24: return csg::resident_kernel_L24(gen, nseg);
         default: return nullptr;
     }
 }
@@ -178,7 +180,7 @@ void fill_launch(cudaLaunchConfig_t& lc, cudaLaunchAttribute* attr, int W, const
                  cudaStream_t st) {
     lc = cudaLaunchConfig_t{};
     lc.gridDim = dim3((unsigned)(W * pl.K), 1, 1);
-    lc.blockDim = dim3((unsigned)(pl.Qc * pl.TPQ), 1, 1);
+    lc.blockDim = dim3((unsigned)pl.threads, 1, 1);
     lc.dynamicSmemBytes = pl.smem;
     lc.stream = st;
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -190,10 +192,12 @@ void fill_launch(cudaLaunchConfig_t& lc, cudaLaunchAttribute* attr, int W, const
 }
 
 // Launch plan: split the G = C*T/4 quads of a word over K = G/Qc CTAs of a
-// cluster.  The score is the number of quads the busiest SM must sweep
-// (waves of co-resident clusters times the quads per SM in a wave); ties go
-// to the smaller cluster (fewer cross-CTA exchanges).
-int make_plan(const csg_config& cfg, bool gen, Plan& out, int forced_qc = 0) {
+// cluster, each quad's team of TPQ = L * L/2 * NSEG threads.  The score is the
+// number of quads the busiest SM must sweep (waves of co-resident clusters
+// times the quads per SM in a wave); ties go to the smaller cluster (fewer
+// cross-CTA exchanges), then to the default column split.  Fields of `forced`
+// (and of the process-wide override) that are non-zero fix that part.
+int make_plan(const csg_config& cfg, bool gen, Plan& out, PlanChoice forced = PlanChoice{}) {
     const int L = cfg.dims.L, W = cfg.dims.n_words;
     const int G = cfg.dims.n_copies * cfg.dims.n_temps / 4;
     if (use_stream(cfg)) {  // fixed launch shapes, nothing to plan
@@ -201,56 +205,59 @@ int make_plan(const csg_config& cfg, bool gen, Plan& out, int forced_qc = 0) {
         out.TPQ = csg::kStreamThreads;
         return CSG_OK;
     }
-    const int tpq = csg::tpq_for(L);
     const bool has_m = gen || (cfg.flags & CSG_MEASURE_M);
-    KernelFn fn = select_kernel(L, gen);
-    if (!fn) return fail(CSG_ERR_UNSUPPORTED, "no kernel for L");
     {
         std::lock_guard<std::mutex> lk(g_plan_mu);
-        if (forced_qc > 0 || g_override.quads_per_cta > 0) {
-            const int Qc = forced_qc > 0 ? forced_qc : g_override.quads_per_cta;
-            if (G % Qc != 0) return fail(CSG_ERR_ARG, "plan override does not divide the quads");
-            out.Qc = Qc;
-            out.K = G / Qc;
-            out.TPQ = tpq;
-            out.smem = smem_for(L, Qc, has_m, gen);
-            if (out.K > 16 || out.smem > kMaxSmem || Qc * tpq > csg::kMaxThreads)
-                return fail(CSG_ERR_UNSUPPORTED, "plan override exceeds device limits");
-            return prepare_kernel(fn, out.smem, out.K);
-        }
+        if (forced.qc == 0) forced.qc = g_override.quads_per_cta;
+        if (forced.nseg == 0 && g_override.threads_per_quad > 0)
+            forced.nseg = g_override.threads_per_quad / (L * (L / 2));
     }
+    if (forced.qc < 0 || forced.nseg < 0) return fail(CSG_ERR_ARG, "negative plan entry");
+    if (forced.qc > 0 && G % forced.qc != 0)
+        return fail(CSG_ERR_ARG, "plan override does not divide the quads");
     int dev = 0, nsm = 0;
     CSG_CUDA(cudaGetDevice(&dev));
     CSG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     long best = -1;
-    for (int Qc = 1; Qc <= G; ++Qc) {
-        if (G % Qc) continue;
-        Plan pl;
-        pl.Qc = Qc;
-        pl.K = G / Qc;
-        pl.TPQ = tpq;
-        pl.smem = smem_for(L, Qc, has_m, gen);
-        if (pl.K > 16 || pl.smem > kMaxSmem || Qc * tpq > csg::kMaxThreads) continue;
-        if (prepare_kernel(fn, pl.smem, pl.K) != CSG_OK) continue;
-        cudaLaunchConfig_t lc;
-        cudaLaunchAttribute attr[1];
-        fill_launch(lc, attr, W, pl, nullptr);
-        int nclusters = 0;
-        if (cudaOccupancyMaxActiveClusters(&nclusters, fn, &lc) != cudaSuccess || nclusters < 1) {
-            cudaGetLastError();
-            continue;
-        }
-        const long waves = (W + nclusters - 1) / nclusters;
-        const long per_wave = (long)std::min(W, nclusters) * pl.K;
-        const long load = waves * ((per_wave + nsm - 1) / nsm) * Qc;
-        const long score = load * 64 + pl.K;
-        if (best < 0 || score < best) {
-            best = score;
-            out = pl;
+    for (int oi = 0; csg::nseg_option(L, oi) > 0; ++oi) {
+        const int nseg = csg::nseg_option(L, oi);
+        if (forced.nseg > 0 && nseg != forced.nseg) continue;
+        KernelFn fn = select_kernel(L, gen, nseg);
+        if (!fn) continue;
+        for (int Qc = 1; Qc <= G; ++Qc) {
+            if (G % Qc || (forced.qc > 0 && Qc != forced.qc)) continue;
+            Plan pl;
+            pl.Qc = Qc;
+            pl.K = G / Qc;
+            pl.NSEG = nseg;
+            pl.TPQ = csg::threads_per_quad(L, nseg);
+            pl.threads = (Qc * pl.TPQ + 31) / 32 * 32;
+            pl.smem = smem_for(L, Qc, has_m, gen);
+            if (pl.K > 16 || pl.smem > kMaxSmem || pl.threads > csg::kMaxThreads) continue;
+            if (prepare_kernel(fn, pl.smem, pl.K) != CSG_OK) continue;
+            cudaLaunchConfig_t lc;
+            cudaLaunchAttribute attr[1];
+            fill_launch(lc, attr, W, pl, nullptr);
+            int nclusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&nclusters, fn, &lc) != cudaSuccess || nclusters < 1) {
+                cudaGetLastError();
+                continue;
+            }
+            const long waves = (W + nclusters - 1) / nclusters;
+            const long per_wave = (long)std::min(W, nclusters) * pl.K;
+            const long load = waves * ((per_wave + nsm - 1) / nsm) * Qc;
+            const long score = (load * 64 + pl.K) * 8 + oi;
+            if (best < 0 || score < best) {
+                best = score;
+                out = pl;
+            }
         }
     }
-    if (best < 0) return fail(CSG_ERR_UNSUPPORTED, "no launch plan fits this configuration");
-    return prepare_kernel(fn, out.smem, out.K);
+    if (best < 0)
+        return fail(CSG_ERR_UNSUPPORTED, forced.qc > 0 || forced.nseg > 0
+                                             ? "plan override exceeds device limits"
+                                             : "no launch plan fits this configuration");
+    return prepare_kernel(select_kernel(L, gen, out.NSEG), out.smem, out.K);
 }
 
 int64_t count_events(int64_t s0, int64_t n, int64_t k, int64_t first_sweep) {
@@ -453,7 +460,7 @@ int run_stream(const csg_config& cfg, uint32_t* spins, const uint32_t* bonds,
 
 int csg_detail::run_device(const csg_config& cfg, uint32_t* spins, const uint32_t* bonds,
                            const csg_device_obs* obs, int64_t sweep0, int64_t n_sweeps,
-                           cudaStream_t st, int forced_qc, long long* sweep_dev,
+                           cudaStream_t st, PlanChoice forced, long long* sweep_dev,
                            const Plan* plan_in) {
     if (use_stream(cfg)) {
         if (sweep_dev)
@@ -466,10 +473,11 @@ int csg_detail::run_device(const csg_config& cfg, uint32_t* spins, const uint32_
     Plan pl;
     if (plan_in)
         pl = *plan_in;  // planned before a stream capture
-    else if (int rc = make_plan(cfg, gen, pl, forced_qc))
+    else if (int rc = make_plan(cfg, gen, pl, forced))
         return rc;
     P.sweep_dev = sweep_dev;
-    KernelFn fn = select_kernel(cfg.dims.L, gen);
+    KernelFn fn = select_kernel(cfg.dims.L, gen, pl.NSEG);
+    if (!fn) return fail(CSG_ERR_UNSUPPORTED, "no resident kernel for this plan");
     P.spins = spins;
     P.bonds = bonds;
     if (obs) {
@@ -506,18 +514,22 @@ int csg_detail::run_device(const csg_config& cfg, uint32_t* spins, const uint32_
 }
 
 
-std::vector<int> csg_detail::quad_splits(const csg_config& c) {
-    std::vector<int> out;
+std::vector<PlanChoice> csg_detail::plan_options(const csg_config& c) {
+    std::vector<PlanChoice> out;
     if (use_stream(c)) return out;
     csg::PtParams P;
     bool gen = false;
     fill_params(c, P, gen);
     const int L = c.dims.L, G = c.dims.n_copies * c.dims.n_temps / 4;
     const bool has_m = gen || (c.flags & CSG_MEASURE_M);
-    for (int qc = 1; qc <= G; ++qc)
-        if (G % qc == 0 && G / qc <= 16 && smem_for(L, qc, has_m, gen) <= kMaxSmem &&
-            qc * csg::tpq_for(L) <= csg::kMaxThreads)
-            out.push_back(qc);
+    for (int oi = 0; csg::nseg_option(L, oi) > 0; ++oi) {
+        const int nseg = csg::nseg_option(L, oi);
+        const int tpq = csg::threads_per_quad(L, nseg);
+        for (int qc = 1; qc <= G; ++qc)
+            if (G % qc == 0 && G / qc <= 16 && smem_for(L, qc, has_m, gen) <= kMaxSmem &&
+                (qc * tpq + 31) / 32 * 32 <= csg::kMaxThreads)
+                out.push_back(PlanChoice{qc, nseg});
+    }
     return out;
 }
 
@@ -525,10 +537,10 @@ int csg_detail::plan_engine(csg_engine* e, Plan& pl, size_t min_smem) {
     csg::PtParams P;
     bool gen = false;
     fill_params(e->cfg, P, gen);
-    if (int rc = make_plan(e->cfg, gen, pl, e->qc)) return rc;
+    if (int rc = make_plan(e->cfg, gen, pl, PlanChoice{e->qc, e->nseg})) return rc;
     if (pl.smem < min_smem && !use_stream(e->cfg)) {
         pl.smem = min_smem;
-        return prepare_kernel(select_kernel(e->cfg.dims.L, gen), pl.smem, pl.K);
+        return prepare_kernel(select_kernel(e->cfg.dims.L, gen, pl.NSEG), pl.smem, pl.K);
     }
     return CSG_OK;
 }
@@ -740,7 +752,8 @@ int csg_run(csg_engine* e, int64_t n_sweeps) {
     if (n_sweeps < 0) return fail(CSG_ERR_ARG, "negative sweep count");
     if (n_sweeps == 0) return CSG_OK;
     const csg_device_obs o = device_obs(e);
-    if (int rc = run_device(e->cfg, e->spins, e->bonds, &o, e->sweep, n_sweeps, e->stream, e->qc))
+    if (int rc = run_device(e->cfg, e->spins, e->bonds, &o, e->sweep, n_sweeps, e->stream,
+                            PlanChoice{e->qc, e->nseg}))
         return rc;
     account(e, n_sweeps);
     return CSG_OK;

@@ -30,7 +30,9 @@ struct csg_engine {
     uint32_t* swap_log = nullptr;
     uint64_t* boundary = nullptr;
     int64_t sweep = 0, n_meas = 0, swap_rounds = 0, swap_round0 = 0;
-    int qc = 0;  // quads per CTA chosen by a batch's tuner (0: automatic plan)
+    // resident-kernel plan chosen by a batch's tuner or a server (0: automatic)
+    int qc = 0;    // quads per CTA
+    int nseg = 0;  // column segments per thread (threads per quad = L * L/2 * nseg)
     // device scratch of csg_obs_records, allocated at its first call
     char* rec_scratch = nullptr;
 };
@@ -40,10 +42,16 @@ struct csg_engine {
 namespace csg_detail {
 
 // Launch shape of the cluster-resident kernel: Qc quads per CTA, K CTAs per
-// cluster (one cluster per sample word), TPQ threads per quad.
+// cluster (one cluster per sample word), TPQ threads per quad (NSEG column
+// segments per thread), CTA of `threads` (Qc*TPQ rounded up to whole warps).
 struct Plan {
-    int Qc = 0, K = 0, TPQ = 0;
+    int Qc = 0, K = 0, TPQ = 0, NSEG = 0, threads = 0;
     size_t smem = 0;
+};
+
+// A resident-kernel plan to force (0 in a field: choose it automatically).
+struct PlanChoice {
+    int qc = 0, nseg = 0;
 };
 
 // Error reporting: the message is what csg_last_error() returns on this thread.
@@ -56,22 +64,22 @@ CSG_INTERNAL int validate(const csg_config* cfg);
 CSG_INTERNAL bool use_stream(const csg_config& c);  // streaming engine, not the resident kernel
 CSG_INTERNAL size_t footprint_bytes(const csg_config& c);
 
-// Quads per CTA that fit one CTA and one cluster of the resident kernel, in
-// increasing order (empty for the streaming engine).
-CSG_INTERNAL std::vector<int> quad_splits(const csg_config& c);
+// The (quads per CTA, column segments) pairs that fit one CTA and one
+// cluster of the resident kernel (empty for the streaming engine).
+CSG_INTERNAL std::vector<PlanChoice> plan_options(const csg_config& c);
 
-// Plan of an engine's resident kernel (its tuner choice e->qc, if any), with
-// the CTA's shared memory raised to at least min_smem.
+// Plan of an engine's resident kernel (its tuner choice e->qc / e->nseg, if
+// any), with the CTA's shared memory raised to at least min_smem.
 CSG_INTERNAL int plan_engine(csg_engine* e, Plan& pl, size_t min_smem = 0);
 
-// n_sweeps sweeps from sweep0 on caller buffers, launched on st.  forced_qc
-// fixes the quads per CTA; sweep_dev (resident kernel only) makes the kernel
+// n_sweeps sweeps from sweep0 on caller buffers, launched on st.  forced
+// fixes parts of the plan; sweep_dev (resident kernel only) makes the kernel
 // read its starting sweep from device memory and advance it, for replayed
 // graphs; plan_in skips planning (required inside a stream capture).
 CSG_INTERNAL int run_device(const csg_config& cfg, uint32_t* spins, const uint32_t* bonds,
                             const csg_device_obs* obs, int64_t sweep0, int64_t n_sweeps,
-                            cudaStream_t st, int forced_qc = 0, long long* sweep_dev = nullptr,
-                            const Plan* plan_in = nullptr);
+                            cudaStream_t st, PlanChoice forced = PlanChoice{},
+                            long long* sweep_dev = nullptr, const Plan* plan_in = nullptr);
 
 CSG_INTERNAL csg_device_obs device_obs(const csg_engine* e);
 

@@ -17,12 +17,16 @@ using namespace csg_detail;
 
 namespace {
 
-// Quads per CTA for a request that shares the GPU with others: the largest
-// split that fits one CTA (fewest CTAs and cluster barriers per unit of work);
-// 0 (the single-request plan) for the streaming engine.
-int shared_gpu_qc(const csg_config& c) {
-    const std::vector<int> s = quad_splits(c);
-    return s.empty() ? 0 : s.back();
+// Plan for a request that shares the GPU with others: the largest split of
+// quads that fits one CTA with the default column split (fewest CTAs and
+// cluster barriers per unit of work); automatic (the single-request plan) for
+// the streaming engine.
+PlanChoice shared_gpu_plan(const csg_config& c) {
+    const std::vector<PlanChoice> opts = plan_options(c);
+    PlanChoice best{};
+    for (const PlanChoice& o : opts)
+        if (o.nseg == opts.front().nseg && o.qc > best.qc) best = o;
+    return best;
 }
 
 }  // namespace
@@ -139,7 +143,9 @@ int csg_server_poll(csg_server* s, int64_t* completed, int32_t max_completed,
         const int64_t n = std::min<int64_t>(s->chunk, r.total - r.launched);
         // alone, a request takes the plan that spreads it widest; sharing the
         // GPU, the one with the fewest CTAs (every plan gives the same bits)
-        r.e->qc = running > 1 ? shared_gpu_qc(r.cfg) : 0;
+        const PlanChoice pc = running > 1 ? shared_gpu_plan(r.cfg) : PlanChoice{};
+        r.e->qc = pc.qc;
+        r.e->nseg = pc.nseg;
         if (int rc = csg_run(r.e, n)) {
             failed(r, rc);
             continue;

@@ -108,6 +108,48 @@ def test_plan_variants_agree(csg, orc, qc):
     _compare_obs(o_gpu, o_orc)
 
 
+# (L, T, quads per CTA, threads per quad): both column splits of each L, and
+# teams that are not whole warps (L = 6, 10, 12, 14), so that warps hold
+# lanes of two quads and padding threads
+TILES = [
+    (6, 8, 1, 36), (6, 8, 4, 36),
+    (8, 8, 4, 32), (8, 8, 2, 64),
+    (10, 8, 1, 50), (10, 8, 4, 100), (10, 8, 2, 50),
+    (12, 16, 4, 72), (12, 16, 2, 144), (12, 16, 1, 72),
+    (14, 20, 5, 98), (14, 20, 2, 98), (14, 20, 2, 196),
+    (16, 24, 3, 128), (16, 24, 2, 256), (16, 24, 1, 128),
+]
+
+
+@pytest.mark.parametrize("L,T,qc,tpq", TILES)
+@pytest.mark.parametrize("H", [0.0, 0.4])
+def test_tile_variants_match_oracle(csg, orc, L, T, qc, tpq, H):
+    """Every tile (quads per CTA x threads per quad) gives the oracle's bits,
+    with exchange and measurement every sweep, at H = 0 and H != 0."""
+    W, C_, n = 1, 2, 6
+    seed = 4242 + L
+    betas = orc.geometric_betas(T, 0.3, 2.0)
+    spins, bonds = orc.init(L, W, C_, T, seed)
+    csg.set_plan_override(qc, tpq)
+    try:
+        plan = csg.query_plan(L, W, C_, betas, H=H)
+        assert (plan.quads_per_cta, plan.threads_per_quad) == (qc, tpq)
+        with csg.Engine(L, W, C_, betas, H=H, seed=seed, sweeps_per_swap=1, sweeps_per_meas=1,
+                        flags=csg.CSG_MEASURE_M, swap_log_rounds=n) as e:
+            e.set_state(spins, bonds, 0)
+            e.run(n)
+            s_gpu, _, _ = e.get_state()
+            o_gpu = e.observables()
+    finally:
+        csg.set_plan_override(None)
+    o_orc = orc.Observables(L, W, C_, T, log_rounds=n)
+    orc.run(spins, bonds, L=L, betas=betas, H=H, seed=seed, sweep0=0, n_sweeps=n,
+            sweeps_per_swap=1, sweeps_per_meas=1, obs=o_orc)
+    np.testing.assert_array_equal(s_gpu, spins)
+    _compare_obs(o_gpu, o_orc, with_m=True)
+    np.testing.assert_array_equal(o_gpu.swap_log[:n], o_orc.swap_log[:n])
+
+
 def test_long_run_crosses_launch_boundary(csg, orc):
     """More sweeps than one launch holds; resumes mid-schedule."""
     L, W, C_, T = 4, 1, 2, 8
