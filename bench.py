@@ -1,16 +1,25 @@
 """Benchmark: spin-flip attempts/ns of the parallel-tempering engine on B200.
 
-Workload (the plain engine at production size): L=16 periodic +-J lattice,
-1024 disorder samples (32 uint32 words x 32 bits), 2 copies, 24 temperatures
-geometric in T in [0.2, 2.0], a replica-exchange attempt every sweep, e and q
-measured every sweep (the measurement half of a 65536-sweep run).  One step is
-one section of 1024 sweeps = one kernel launch.  Synthetic, seeded disorder.
+Default workload (the headline line): the batched engine on uneven sizes —
+L=12 x 512 disorder samples (16 temperatures), L=14 x 384 (20), L=16 x 256
+(24), 2 copies each, temperatures geometric in T=[0.2, 2.0], seeded +-J
+disorder, uniform random initial spins — advanced as one captured CUDA graph
+per step (1024 sweeps of every member), tile plans chosen by the autotuner,
+with the reference program's schedule (exchange every 16 sweeps, measurement
+every 1024).  The same run measures, in the same line: the every-sweep
+schedule, the plain engine looping over the same lattices (both schedules),
+the end-to-end rate through the csg_batch_* API with host state in and
+observables out, the production shape (L=16, 1024 samples, 24 temperatures,
+exchange and measurement every sweep), a short serving run (p50/p99 against a
+stated p99 objective), the CPU oracle on the host cores, and the reference's
+own CUDA program on this GPU.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload mixed|production|serving|large]
 
-Prints one JSON line (rank 0).  With torchrun, the ranks share one simulation
-of N x 1024 samples, 1024 per rank (sample words sharded with word0; weak
-scaling, no collective on the data path).
+Prints one JSON line (rank 0).  With torchrun each rank runs its own shard of
+sample words of every member (word0 offsets; weak scaling, no collective on
+the data path); the time is the max over ranks.
 """
 from __future__ import annotations
 
@@ -136,8 +145,14 @@ def int_peak_ops() -> dict:
             "(spin-glass_b200/csrc/int_peak.cu), best of 5, in this run"}
 
 
+PROFILE_TRAFFIC_SOURCE = ("constant from the committed ncu summary "
+                          "profiles/pt_resident_L16_production.json (dram__bytes_read.sum + "
+                          "dram__bytes_write.sum of one resident-kernel launch of the production "
+                          "shape); not measured in this run")
+
+
 def profile_traffic():
-    """DRAM bytes per launch of the sweep kernel from the committed ncu summary."""
+    """DRAM bytes per launch of the resident kernel from the committed ncu summary."""
     f = ROOT / "profiles" / "pt_resident_L16_production.json"
     if not f.exists():
         return None
@@ -223,32 +238,57 @@ def reference_cuda_baseline(timeout_s: float = 300.0) -> dict:
 
 
 def run_reference(args, rank: int, world: int) -> None:
+    """The reference arm: the reference's update rule as restated by the CPU
+    oracle (the reference program itself is CUDA-only and has no CPU path), on
+    all host cores, on our arm's workload and schedule.  Rank 0 alone runs it;
+    each step is a bounded sample of the workload (REF_STEP_SWEEPS sweeps of
+    every member for the batched workload, one sweep for the production
+    shape)."""
     if rank != 0:
         return
     from oracle import oracle as orc
     orc.build()
-    betas = 1.0 / (T_MIN * (T_MAX / T_MIN) ** (np.arange(T) / (T - 1)))
-    spins, bonds = orc.init(L, W, NCOPY, T, SEED)
-    obs = orc.Observables(L, W, NCOPY, T)
-    # one step = one sweep of the workload (a bounded sample of a 1024-sweep section)
-    for k in range(args.warmup):
-        orc.run(spins, bonds, L=L, betas=betas, H=0.0, seed=SEED, sweep0=SWEEP0 + k,
-                n_sweeps=1, sweeps_per_swap=1, sweeps_per_meas=1, obs=obs)
-    t0 = time.perf_counter()
-    orc.run(spins, bonds, L=L, betas=betas, H=0.0, seed=SEED, sweep0=SWEEP0 + args.warmup,
-            n_sweeps=args.steps, sweeps_per_swap=1, sweeps_per_meas=1, obs=obs)
-    el = time.perf_counter() - t0
-    value = args.steps * attempts_per_sweep() / (el * 1e9)
     cores = os.cpu_count()
+    if args.workload == "production":
+        state = [(dict(L=L, n_words=W, betas=ladder(T), seed=SEED), 1, 1)]
+        step_sweeps, config = 1, workload_config(world)
+        words = W * NCOPY * T * L ** 3
+    else:
+        sps = args.swap_every if args.swap_every is not None else REF_SCHEDULE[0]
+        spm = args.measure_every if args.measure_every is not None else REF_SCHEDULE[1]
+        state = [(m, sps, spm) for m in mixed_members(sps, spm)]
+        step_sweeps, config = REF_STEP_SWEEPS, mixed_config(world, sps, spm)
+        words = MIXED_WORDS_PER_SWEEP
+    sims = []
+    for m, sps, spm in state:
+        T_ = len(m["betas"])
+        s_, b_ = orc.init(m["L"], m["n_words"], NCOPY, T_, m["seed"])
+        sims.append((m, sps, spm, s_, b_, orc.Observables(m["L"], m["n_words"], NCOPY, T_)))
+
+    def step(k):
+        for m, sps, spm, s_, b_, o_ in sims:
+            orc.run(s_, b_, L=m["L"], betas=m["betas"], H=0.0, seed=m["seed"],
+                    sweep0=SWEEP0 + k * step_sweeps, n_sweeps=step_sweeps, sweeps_per_swap=sps,
+                    sweeps_per_meas=spm, obs=o_)
+
+    for k in range(args.warmup):
+        step(k)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        step(args.warmup + k)
+    el = time.perf_counter() - t0
+    value = args.steps * step_sweeps * words * 32 / (el * 1e9)
+    sample = (f"{args.steps} steps of {step_sweeps} sweep(s) of every member of the workload, "
+              f"{cores} OpenMP threads; the reference itself has no CPU implementation of "
+              "this path, so its update rule runs as restated by the oracle")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": workload_config(world),
+            "ms_per_step": el * 1e3 / args.steps, "sweeps_per_step": step_sweeps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded +-J disorder, uniform random initial spins)",
+            "config": config,
             "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "port",
-                             "sample": f"{args.steps} sweeps of the workload (1 sweep per step), "
-                                       f"{cores} OpenMP threads; the reference itself has no "
-                                       "CPU implementation of this path"},
+                             "sample": sample},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -261,7 +301,7 @@ def run_ours(args, rank: int, world: int, dist) -> None:
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     seed = SEED  # one simulation of world x 1024 samples, sharded by sample word
-    betas = 1.0 / (T_MIN * (T_MAX / T_MIN) ** (np.arange(T) / (T - 1)))
+    betas = ladder(T)
     cfg, _keep = csg.make_config(L, W, NCOPY, betas, H=args.field, seed=seed,
                                  sweeps_per_swap=args.swap_every,
                                  sweeps_per_meas=args.measure_every, meas_start=0, word0=rank * W,
@@ -381,80 +421,267 @@ def run_e2e(csg, torch, betas, seed, args, word0: int = 0) -> dict:
 
 MIXED = [  # L, sample words, temperatures (batched, uneven sizes; 2 copies each)
     (12, 16, 16), (14, 12, 20), (16, 8, 24)]
-
-
 REF_SCHEDULE = (16, 1024)  # the reference program's SBSHFL, SBMEAS (eamsim.cuh:20-21)
+# word updates per mixed-workload sweep (32 attempts each)
+MIXED_WORDS_PER_SWEEP = sum(l ** 3 * w * NCOPY * t for l, w, t in MIXED)
+REF_STEP_SWEEPS = 64  # CPU reference arm: sweeps of every member per step (a bounded sample)
 
 
-def _mixed_once(csg, args, sps: int, spm: int) -> dict:
-    members = [dict(L=l, n_words=w, n_copies=NCOPY,
-                    betas=1.0 / (T_MIN * (T_MAX / T_MIN) ** (np.arange(t) / (t - 1))),
-                    seed=SEED + l, sweeps_per_swap=sps, sweeps_per_meas=spm)
-               for l, w, t in MIXED]
-    per_sweep = sum(l ** 3 * w * 32 * NCOPY * t for l, w, t in MIXED)
+def ladder(t: int, lo: float = T_MIN, hi: float = T_MAX) -> np.ndarray:
+    """Inverse temperatures of t temperatures geometric in [lo, hi]; plane 0 coldest."""
+    return 1.0 / (lo * (hi / lo) ** (np.arange(t) / (t - 1)))
+
+
+def mixed_members(sps: int, spm: int, rank: int = 0) -> list:
+    """The batched workload's members; rank r simulates sample words
+    [r W, (r+1) W) of each member (its shard of a world x larger run)."""
+    return [dict(L=l, n_words=w, n_copies=NCOPY, betas=ladder(t), seed=SEED + l,
+                 sweeps_per_swap=sps, sweeps_per_meas=spm, meas_start=0, word0=rank * w)
+            for l, w, t in MIXED]
+
+
+def schedule_name(sps: int, spm: int) -> str:
+    if (sps, spm) == REF_SCHEDULE:
+        return "reference program's (exchange every 16 sweeps, measurement every 1024)"
+    if (sps, spm) == (1, 1):
+        return "every sweep (exchange and measurement)"
+    return f"exchange every {sps}, measurement every {spm}"
+
+
+def mixed_config(world: int, sps: int, spm: int) -> dict:
+    return {"workload": "batched, uneven sizes: L=12 x512, L=14 x384, L=16 x256 samples",
+            "members": [{"L": l, "samples": 32 * w, "temperatures": t} for l, w, t in MIXED],
+            "copies": NCOPY, "T_range": [T_MIN, T_MAX], "field_H": 0.0,
+            "disorder": "+-J bimodal p=1/2 per sample, seeded; uniform random initial spins",
+            "swap_every": sps, "measure_every": spm, "schedule": schedule_name(sps, spm),
+            "l2": "GPU arm: flushed between timed steps (256 MiB write)",
+            "parallelism": f"sample shards x{world}"}
+
+
+def _time_launches(torch, dev, stream, flush, dist, steps, warmup, launch):
+    """Device time of `steps` launches (CUDA events on the launching stream, L2
+    flushed before each), barrier + synchronize on both sides, max over ranks."""
+    for k in range(warmup):
+        launch(k)
+    torch.cuda.synchronize(dev)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
+    for k in range(steps):
+        flush.fill_(k)
+        ev[k][0].record(stream)
+        launch(warmup + k)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    per = [a.elapsed_time(b) for a, b in ev]
+    t_ms = sum(per)
+    if dist is not None:
+        t = torch.tensor([t_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ms = float(t.item())
+    return t_ms, per
+
+
+def _batch_e2e(torch, b, steps: int) -> dict:
+    """End to end through the batch API, wall clock: per step every member's
+    state goes in from pinned host memory (csg_set_state), the batch runs 1024
+    sweeps (csg_batch_run) and every member's observables come back
+    (csg_get_observables)."""
+    hosts = []
+    for e in b.members:
+        s, bd, _ = e.get_state()
+        hs = torch.empty(s.size, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+        hb = torch.empty(bd.size, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+        hs[:] = s.ravel()
+        hb[:] = bd.ravel()
+        hosts.append((hs.reshape(s.shape), hb.reshape(bd.shape)))
+
+    def step(k):
+        for e, (hs, hb) in zip(b.members, hosts):
+            e.set_state(hs, hb, SWEEP0 + k * SWEEPS_PER_STEP)
+        b.run(SWEEPS_PER_STEP)
+        return [e.observables() for e in b.members]
+
+    step(0)  # untimed: first graph capture for this sweep count
+    t0 = time.perf_counter()
+    for k in range(steps):
+        obs = step(k)
+    el = time.perf_counter() - t0
+    d2h = sum(getattr(o, f).nbytes for o in obs
+              for f in ("e_sum", "m_sum", "q_sum", "q2_sum", "q4_sum", "hist", "e_last",
+                        "m_last", "d_last", "swap_acc")) + 8 * len(obs)
+    h2d = sum(hs.nbytes + hb.nbytes for hs, hb in hosts)
+    return {"seconds": el, "attempts": steps * SWEEPS_PER_STEP * MIXED_WORDS_PER_SWEEP * 32,
+            "h2d": int(h2d), "d2h": int(d2h)}
+
+
+def measure_mixed(csg, torch, dev, stream, flush, dist, args, sps, spm, rank, e2e=False,
+                  clocks=False) -> dict:
+    """Batched graph vs the plain engine on the mixed workload at one schedule."""
+    members = mixed_members(sps, spm, rank)
     with csg.Batch(members) as b:
         for e in b.members:
             e.init_lattice()
-        chosen = b.tune(64)
-        for k in range(args.warmup):
-            b.run(SWEEPS_PER_STEP)
-        with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
-            t0 = time.perf_counter()
-            for k in range(args.steps):
-                b.run(SWEEPS_PER_STEP)
-            batched_s = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        for k in range(args.steps):
-            b.run_sequential(SWEEPS_PER_STEP)
-        plain_s = time.perf_counter() - t0
-        b.set_plan([0] * len(members))  # the plain engine with its own per-member plans
-        t0 = time.perf_counter()
-        for k in range(args.steps):
-            b.run_sequential(SWEEPS_PER_STEP)
-        plain_auto_s = time.perf_counter() - t0
-    att = args.steps * SWEEPS_PER_STEP * per_sweep
-    return {"value": att / (batched_s * 1e9), "ms_per_step": batched_s * 1e3 / args.steps,
-            "swap_every": sps, "measure_every": spm,
-            "plain_value": att / (plain_auto_s * 1e9),
-            "plain_value_tuned_plans": att / (plain_s * 1e9),
-            "batched_over_plain": plain_auto_s / batched_s,
-            "quads_per_cta_tuned": [int(q) for q in chosen], "clocks": clk.summary()}
+        b.tune(64)
+        plans = [b.member_plan(i) for i in range(len(members))]
+        clk = ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) if clocks else None
+        if clk:
+            clk.__enter__()
+        t_b, per_b = _time_launches(torch, dev, stream, flush, dist, args.steps, args.warmup,
+                                    lambda k: b.launch(SWEEPS_PER_STEP, stream.cuda_stream))
+        if clk:
+            clk.__exit__()
+        t_p, _ = _time_launches(torch, dev, stream, flush, dist, args.steps, 1,
+                                lambda k: b.launch(SWEEPS_PER_STEP, stream.cuda_stream, plain=True))
+        out = {"t_batched_ms": t_b, "per_launch_ms": per_b, "t_plain_ms": t_p,
+               "plans": [{"L": m["L"], "quads_per_cta": p.quads_per_cta,
+                          "ctas_per_word": p.ctas_per_word, "threads_per_quad": p.threads_per_quad,
+                          "smem_bytes": p.smem_bytes} for m, p in zip(members, plans)],
+               "clocks": clk.summary() if clk else None}
+        if e2e:
+            out["e2e"] = _batch_e2e(torch, b, args.steps)
+    return out
 
 
-def run_mixed(args) -> None:
-    """Batched engine on the mixed L=12/14/16 workload vs the plain engine
-    looping over the same lattices (one step = 1024 sweeps of every member).
-    The headline uses the reference program's own schedule (exchange every 16
-    sweeps, measurement every 1024) unless --swap-every / --measure-every are
-    given; the every-sweep schedule is measured beside it."""
+def mixed_summary(m: dict, world: int, steps: int) -> dict:
+    att = world * steps * SWEEPS_PER_STEP * MIXED_WORDS_PER_SWEEP * 32
+    return {"value": att / (m["t_batched_ms"] * 1e6), "ms_per_step": m["t_batched_ms"] / steps,
+            "plain_value": att / (m["t_plain_ms"] * 1e6),
+            "plain_ms_per_step": m["t_plain_ms"] / steps,
+            "batched_over_plain": m["t_plain_ms"] / m["t_batched_ms"], "tuned_plans": m["plans"]}
+
+
+def int_roofline(words_per_launch: float, per_launch_ms: list, peak: dict) -> dict:
+    mean_s = statistics.mean(per_launch_ms) * 1e-3
+    achieved = words_per_launch * OPS_PER_WORD_UPDATE / mean_s
+    return {"bound": "int", "achieved": achieved / 1e12, "peak": peak["ops_per_s"] / 1e12,
+            "unit": "Tops/s (32-bit integer logic)", "frac": achieved / peak["ops_per_s"],
+            "ops_per_attempt": OPS_PER_WORD_UPDATE / 32, "peak_source": peak["source"],
+            "launch_ms": mean_s * 1e3}
+
+
+def cpu_sample_mixed(target_s: float, sps: int, spm: int) -> dict:
+    """The CPU oracle (a scalar port of the reference's update rule, OpenMP
+    over planes, all host cores) on the mixed workload's members, for a
+    bounded number of sweeps."""
+    from oracle import oracle as orc
+    orc.build()
+    state = []
+    for m in mixed_members(sps, spm):
+        T_ = len(m["betas"])
+        s_, b_ = orc.init(m["L"], m["n_words"], NCOPY, T_, m["seed"])
+        state.append((m, s_, b_, orc.Observables(m["L"], m["n_words"], NCOPY, T_)))
+    sweeps, t0 = 0, time.perf_counter()
+    while True:
+        for m, s_, b_, o_ in state:
+            orc.run(s_, b_, L=m["L"], betas=m["betas"], H=0.0, seed=m["seed"],
+                    sweep0=SWEEP0 + sweeps, n_sweeps=16, sweeps_per_swap=sps,
+                    sweeps_per_meas=spm, obs=o_)
+        sweeps += 16
+        el = time.perf_counter() - t0
+        if el >= target_s:
+            break
+    cores = os.cpu_count()
+    return {"value": sweeps * MIXED_WORDS_PER_SWEEP * 32 / (el * 1e9), "unit": METRIC,
+            "cores": cores, "kind": "port",
+            "sample": f"{sweeps} sweeps of every member of the same workload and schedule, "
+                      f"{el:.1f} s, {cores} OpenMP threads"}
+
+
+def measure_production(csg, torch, dev, stream, flush, args) -> dict:
+    """The plain engine at production size (L=16, 1024 samples, 2 copies, 24
+    temperatures in T=[0.2,2], exchange and measurement every sweep), one
+    1024-sweep launch per step, device-timed."""
+    betas = ladder(T)
+    cfg, _keep = csg.make_config(L, W, NCOPY, betas, seed=SEED, sweeps_per_swap=1,
+                                 sweeps_per_meas=1)
+    N = L ** 3
+    spins = torch.empty(W * NCOPY * T * N, dtype=torch.int32, device=dev)
+    bonds = torch.empty(W * 3 * N, dtype=torch.int32, device=dev)
+    z64 = lambda *s: torch.zeros(s, dtype=torch.int64, device=dev)
+    acc = {"e_sum": z64(W, NCOPY, T, 32), "q_sum": z64(W, T, 32), "q2_sum": z64(W, T, 32),
+           "q4_sum": z64(W, T, 32, 2), "hist": torch.zeros((T, N + 1), dtype=torch.int32, device=dev),
+           "boundary": z64(1)}
+    obs = csg.DeviceObs(**{k: v.data_ptr() for k, v in acc.items()})
+    csg.init_device(cfg, spins.data_ptr(), bonds.data_ptr(), stream.cuda_stream)
+    plan = csg.query_plan(L, W, NCOPY, betas)
+    t_ms, per = _time_launches(
+        torch, dev, stream, flush, None, args.steps, args.warmup,
+        lambda k: csg.run_device(cfg, spins.data_ptr(), bonds.data_ptr(), obs,
+                                 SWEEP0 + k * SWEEPS_PER_STEP, SWEEPS_PER_STEP, stream.cuda_stream))
+    att = args.steps * SWEEPS_PER_STEP * attempts_per_sweep()
+    return {"config": workload_config(1), "value": att / (t_ms * 1e6),
+            "ms_per_step": t_ms / args.steps,
+            "roofline": int_roofline(SWEEPS_PER_STEP * W * NCOPY * T * N, per, int_peak_ops()),
+            "plan": {"quads_per_cta": plan.quads_per_cta, "ctas_per_word": plan.ctas_per_word,
+                     "threads_per_quad": plan.threads_per_quad},
+            "exchange_boundary_cases": int(acc["boundary"].item())}
+
+
+def run_mixed(args, rank: int, world: int, dist) -> None:
+    """The headline line: the batched engine on the mixed L=12/14/16 workload."""
+    import torch
     csg = _package()
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device=dev)  # 256 MiB > L2
     sps = args.swap_every if args.swap_every is not None else REF_SCHEDULE[0]
     spm = args.measure_every if args.measure_every is not None else REF_SCHEDULE[1]
-    main = _mixed_once(csg, args, sps, spm)
-    every = _mixed_once(csg, args, 1, 1) if (sps, spm) != (1, 1) else None
-    ops = OPS_PER_WORD_UPDATE / 32 * main["value"] * 1e9
+    main_m = measure_mixed(csg, torch, dev, stream, flush, dist, args, sps, spm, rank,
+                           e2e=not args.no_e2e, clocks=True)
+    every_m = (measure_mixed(csg, torch, dev, stream, flush, dist, args, 1, 1, rank)
+               if (sps, spm) != (1, 1) else None)
+    e2e_value = None
+    if "e2e" in main_m:
+        secs = main_m["e2e"]["seconds"]
+        if dist is not None:
+            t = torch.tensor([secs], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            secs = float(t.item())
+        e2e_value = world * main_m["e2e"]["attempts"] / (secs * 1e9)
+    if rank != 0:
+        return
     peak = int_peak_ops()
-    line = {"metric": METRIC, "value": main["value"], "unit": METRIC, "n_gpus": 1,
-            "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": main["ms_per_step"], "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": "batched, uneven sizes (L=12 x512, L=14 x384, L=16 x256 "
-                                   "samples; 16/20/24 temperatures in T=[0.2,2]; 2 copies)",
-                       "sweeps_per_step": SWEEPS_PER_STEP, "swap_every": sps,
-                       "measure_every": spm,
-                       "schedule": "reference program's (SBSHFL=16, SBMEAS=1024)"
-                                   if (sps, spm) == REF_SCHEDULE else "given",
-                       "timing": "host clock around synchronous graph launches",
-                       "quads_per_cta_tuned": main["quads_per_cta_tuned"]},
-            "roofline": {"bound": "int", "achieved": ops / 1e12, "peak": peak["ops_per_s"] / 1e12,
-                         "unit": "Tops/s (32-bit integer logic)", "frac": ops / peak["ops_per_s"],
-                         "traffic": None, "ops_per_attempt": OPS_PER_WORD_UPDATE / 32,
-                         "peak_source": peak["source"]},
-            "plain_value": main["plain_value"],
-            "plain_value_tuned_plans": main["plain_value_tuned_plans"],
-            "batched_over_plain": main["batched_over_plain"],
-            "every_sweep_schedule": every,
-            "clocks": main["clocks"]}
+    head = mixed_summary(main_m, world, args.steps)
+    words_per_launch = SWEEPS_PER_STEP * MIXED_WORDS_PER_SWEEP
+    roof = int_roofline(words_per_launch, main_m["per_launch_ms"], peak)
+    roof.update({"kernel": "the batch graph: the members' pt_resident_kernel launches running "
+                           "side by side (one graph launch per step)",
+                 "traffic": profile_traffic(), "traffic_source": PROFILE_TRAFFIC_SOURCE})
+    line = {"metric": METRIC, "value": head["value"], "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
+            "sweeps_per_step": SWEEPS_PER_STEP, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded +-J disorder, uniform random initial spins)",
+            "config": mixed_config(world, sps, spm), "roofline": roof,
+            "plain_value": head["plain_value"], "batched_over_plain": head["batched_over_plain"],
+            "tuned_plans": head["tuned_plans"],
+            "e2e": {"value": e2e_value, "unit": METRIC,
+                    "h2d_bytes_per_step": main_m.get("e2e", {}).get("h2d", 0),
+                    "d2h_bytes_per_step": main_m.get("e2e", {}).get("d2h", 0),
+                    "path": "csg_set_state (pinned host) + csg_batch_run + csg_get_observables, "
+                            "every member, every step; wall clock"},
+            # per step one graph launch: each member's resident kernel and its
+            # sweep-counter kernel
+            "gpu_launches": args.steps * 2 * len(MIXED),
+            "clocks": main_m["clocks"]}
+    if every_m is not None:
+        ev = mixed_summary(every_m, world, args.steps)
+        ev["roofline_frac"] = int_roofline(words_per_launch, every_m["per_launch_ms"], peak)["frac"]
+        ev["schedule"] = schedule_name(1, 1)
+        line["every_sweep_schedule"] = ev
+    if world == 1 and not args.no_cpu_baseline:
+        line["production"] = measure_production(csg, torch, dev, stream, flush, args)
+        line["serving"] = serving_summary(csg, args)
+        line["cpu_baseline"] = cpu_sample_mixed(args.cpu_seconds, sps, spm)
+        line["reference_cuda"] = reference_cuda_baseline()
     print(json.dumps(line), flush=True)
 
 
@@ -591,8 +818,19 @@ def run_large(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+# Serving objective: at the default arrival rate (2 requests/s), the 99th
+# percentile of completion latency (arrival to result) stays within this bound.
+# The largest request the stream can draw (L=16, 1024 samples, 32
+# temperatures, 65536 sweeps) alone takes about 2.5 s on the GPU.
+SERVE_SLO_P99_S = 4.0
+
+
 def _serve_requests(args, rate):
-    """The request stream: arrival times (rate None: all at once) and configs."""
+    """The request stream: arrival times (rate None: all at once) and configs.
+    Each request: L in {8..16} even, 32..1024 samples (multiples of 32), 16..32
+    temperatures (multiples of 4) geometric in T=[0.2,2], 4096..65536 sweeps
+    (multiples of 1024), its own seed; exchange every sweep, measurement every
+    16 sweeps in the second half (the first half thermalises)."""
     rng = np.random.default_rng(args.serve_seed)
     n_req = args.serve_requests
     gaps = rng.exponential(1.0 / args.serve_rate, n_req)
@@ -605,10 +843,9 @@ def _serve_requests(args, rate):
         w = int(rng.integers(1, 33))
         t = int(rng.choice([16, 20, 24, 28, 32]))
         sweeps = 1024 * int(rng.integers(4, 65))
-        betas = 1.0 / (T_MIN * (T_MAX / T_MIN) ** (np.arange(t) / (t - 1)))
-        reqs.append((arrivals[i], sweeps, dict(L=L_, n_words=w, n_copies=NCOPY, betas=betas,
+        reqs.append((arrivals[i], sweeps, dict(L=L_, n_words=w, n_copies=NCOPY, betas=ladder(t),
                                                seed=SEED + 7919 * i, sweeps_per_swap=1,
-                                               sweeps_per_meas=0)))
+                                               sweeps_per_meas=16, meas_start=sweeps // 2)))
     work = sum(r[1] * r[2]["L"] ** 3 * r[2]["n_words"] * 32 * NCOPY * len(r[2]["betas"])
                for r in reqs)
     return reqs, work
@@ -660,28 +897,42 @@ def _serve_sequential(csg, args) -> dict:
     return {"value": work / (el * 1e9), "seconds": el}
 
 
-def run_serving(args) -> None:
-    """Poisson request stream through the continuous-batching server: each
-    request draws L in {8..16} (even), 32..1024 samples (multiples of 32),
-    16..32 temperatures (multiples of 4) geometric in T=[0.2,2], 4096..65536
-    sweeps (multiples of 1024), seeded +-J disorder; exchange every sweep.
-    Beside the stated arrival rate (latency): the same requests all at once
-    (throughput of continuous batching) and on the plain engine one after
-    another."""
-    csg = _package()
+def serving_config(args) -> dict:
+    return {"workload": "serving stream, Poisson arrivals",
+            "rate_per_s": args.serve_rate, "requests": args.serve_requests,
+            "memory_budget_GiB": args.serve_budget_gb, "max_active": args.serve_slots,
+            "seed": args.serve_seed,
+            "request": "L in {8..16}, 32-1024 samples, 16-32 temperatures in T=[0.2,2], "
+                       "4096-65536 sweeps; exchange every sweep, measurement every 16 "
+                       "sweeps in the second half"}
+
+
+def serving_summary(csg, args) -> dict:
+    """One pass of the request stream at the stated rate: p50/p99 completion
+    latency against the p99 objective, and the aggregate rate."""
     main = _serve_once(csg, args, args.serve_rate)
+    return {"config": serving_config(args), "value": main["value"], "unit": METRIC,
+            "latency_s": main["latency_s"], "slo": {"p99_s": SERVE_SLO_P99_S,
+                                                    "met": main["latency_s"]["p99"] <= SERVE_SLO_P99_S},
+            "makespan_s": main["makespan_s"], "peak_active": main["peak_active"],
+            "timing": "host wall clock, arrival to result fetched",
+            "note": "at this arrival rate the aggregate rate is bounded by the arrivals"}
+
+
+def run_serving(args) -> None:
+    """Poisson request stream through the continuous-batching server, the
+    same requests all at once (throughput of continuous batching), and the
+    plain engine running them one after another."""
+    csg = _package()
+    main = serving_summary(csg, args)
     burst = _serve_once(csg, args, None)
     seq = _serve_sequential(csg, args)
     line = {"metric": "serving: " + METRIC + " with p50/p99 completion latency",
             "value": main["value"], "unit": METRIC, "n_gpus": 1,
             "higher_is_better": True, "dtype": "u32", "data": "synthetic",
-            "latency_s": main["latency_s"],
-            "config": {"workload": "serving stream, Poisson arrivals",
-                       "rate_per_s": args.serve_rate, "requests": args.serve_requests,
-                       "memory_budget_GiB": args.serve_budget_gb, "max_active": args.serve_slots,
-                       "seed": args.serve_seed, "total_attempts": main["total_attempts"],
-                       "makespan_s": main["makespan_s"], "peak_active": main["peak_active"],
-                       "note": "at this rate the value is bounded by the arrivals"},
+            "latency_s": main["latency_s"], "slo": main["slo"],
+            "config": dict(main["config"], makespan_s=main["makespan_s"],
+                           peak_active=main["peak_active"]),
             "all_at_once": burst,
             "plain_engine_one_after_another": seq,
             "batched_over_plain": burst["value"] / seq["value"]}
@@ -695,13 +946,15 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the CPU oracle, the reference's CUDA program and the "
+                         "production and serving sub-runs of the default line")
     ap.add_argument("--swap-every", type=int, default=None,
-                    help="sweeps per exchange round (0: none; default 1, mixed: 16)")
+                    help="sweeps per exchange round (0: none; default: mixed 16, production 1)")
     ap.add_argument("--measure-every", type=int, default=None,
-                    help="sweeps per measurement (0: none; default 1, mixed: 1024)")
-    ap.add_argument("--workload", choices=["production", "mixed", "serving", "large"],
-                    default="production")
+                    help="sweeps per measurement (0: none; default: mixed 1024, production 1)")
+    ap.add_argument("--workload", choices=["mixed", "production", "serving", "large"],
+                    default="mixed")
     ap.add_argument("--field", type=float, default=0.0,
                     help="production workload: external field H (H != 0: general-field kernel)")
     ap.add_argument("--engine", choices=["auto", "stream"], default="auto",
@@ -712,7 +965,8 @@ def main() -> None:
     ap.add_argument("--serve-slots", type=int, default=32)
     ap.add_argument("--serve-seed", type=int, default=5)
     ap.add_argument("--sweeps-per-step", type=int, default=None,
-                    help="sweeps per timed step (default 1024; large workload 256)")
+                    help="production / large workloads: sweeps per timed step "
+                         "(default 1024; large 256)")
     ap.add_argument("--large-L", type=int, choices=[32, 48], default=None,
                     help="large workload: one lattice size only")
     ap.add_argument("--no-e2e", action="store_true",
@@ -720,19 +974,14 @@ def main() -> None:
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
-    dist = None
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
     if args.sweeps_per_step is None:
         args.sweeps_per_step = LARGE_SWEEPS_PER_STEP if args.workload == "large" else SWEEPS_PER_STEP
-    if args.workload != "mixed":
+    if args.workload == "production":
         args.swap_every = 1 if args.swap_every is None else args.swap_every
         args.measure_every = 1 if args.measure_every is None else args.measure_every
-    if args.workload == "mixed":
-        if rank == 0:
-            run_mixed(args)
-        return
     if args.workload == "serving":
         if rank == 0:
             run_serving(args)
@@ -741,13 +990,19 @@ def main() -> None:
         if rank == 0:
             run_large(args)
         return
+    dist = None
     if world > 1:
         import datetime
 
+        import torch
         import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     try:
-        run_ours(args, rank, world, dist)
+        if args.workload == "mixed":
+            run_mixed(args, rank, world, dist)
+        else:
+            run_ours(args, rank, world, dist)
     finally:
         if dist is not None:
             dist.destroy_process_group()

@@ -167,9 +167,12 @@ int csg_get_observables(csg_engine* e, csg_observables* out);
 int csg_reset_observables(csg_engine* e);
 
 /* rearrange + compute_q (eamsim.cu:419-511) and the e/m output of
- * eamsim.cu:407-415: observable records obs_s (eamsim.cuh:55-62) of the
- * current state, 11 floats {e[2], m[2], q_0, q_1_r[3], q_1_i[3]} per
- * (sample, temperature), shape [32W][T][11].  Requires n_copies == 2. */
+ * eamsim.cu:407-415: observable records obs_s (eamsim.cuh:55-62), 11 floats
+ * {e[2], m[2], q_0, q_1_r[3], q_1_i[3]} per (sample, temperature), shape
+ * [32W][T][11].  Requires n_copies == 2.  All fields are of the current
+ * state; the reference's e/m are those of its last exchange round (taken
+ * before that round's swap, 16 sweeps before the section ends), its q fields
+ * are of the current state as here. */
 int csg_obs_records(csg_engine* e, float* rec, size_t n_floats);
 
 /* eamsim::save_checkpoint / load_checkpoint (eamsim.cu:655-676): the

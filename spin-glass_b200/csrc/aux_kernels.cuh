@@ -6,6 +6,10 @@
 //                   integers of the current state, including the overlap
 //                   summed per coordinate plane, from which the Fourier
 //                   overlaps of compute_q (eamsim.cu:451-511) are formed.
+// records_kernel  : the reference's obs_s records from those integers.
+// The kernels have internal linkage: each translation unit that launches
+// them (the engine, the no-allocation records entry point) has its own copy
+// of the same code.
 #pragma once
 #include <cstdint>
 
@@ -13,7 +17,7 @@
 
 namespace csg {
 
-__global__ void init_kernel(uint32_t* spins, uint32_t* bonds, int L, int W, int C, int Q,
+static __global__ void init_kernel(uint32_t* spins, uint32_t* bonds, int L, int W, int C, int Q,
                             uint32_t k0, uint32_t k1, uint32_t word0) {
     const long N = (long)L * L * L;
     const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -41,7 +45,7 @@ __global__ void init_kernel(uint32_t* spins, uint32_t* bonds, int L, int W, int 
 //   d[w][t][b] = #sites where the copies differ,
 //   dpl[w][t][b][dir][a] = same restricted to coordinate dir == a.
 // Requires two copies. Shared memory: 32 * 3L ints per warp.
-__global__ void measure_kernel(const uint32_t* __restrict__ spins, const uint32_t* __restrict__ bonds,
+static __global__ void measure_kernel(const uint32_t* __restrict__ spins, const uint32_t* __restrict__ bonds,
                                int L, int W, int T, int* e, int* m, int* d, int* dpl) {
     extern __shared__ int sh[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -98,7 +102,7 @@ __global__ void measure_kernel(const uint32_t* __restrict__ spins, const uint32_
 // the same order; cosv/sinv hold cos(k a), sin(k a), k = 2 pi / L, computed on
 // the host.  Built without contraction (-fmad=false), the records equal the
 // host's bit for bit.
-__global__ void records_kernel(const int* __restrict__ e, const int* __restrict__ m,
+static __global__ void records_kernel(const int* __restrict__ e, const int* __restrict__ m,
                                const int* __restrict__ d, const int* __restrict__ dpl,
                                const double* __restrict__ cosv, const double* __restrict__ sinv,
                                int L, int W, int T, float H, float* __restrict__ rec) {

@@ -178,10 +178,10 @@ int csg_batch_create(const csg_config* cfgs, int32_t n, csg_batch** out) {
 int csg_batch_destroy(csg_batch* b) {
     if (!b) return CSG_OK;
     if (b->main) cudaStreamSynchronize(b->main);
-    drop_graphs(b);
+    // a launch on a caller's stream is waited for through the members' streams,
+    // which csg_engine_destroy synchronises
     for (csg_engine* e : b->eng) csg_engine_destroy(e);
-    for (csg_engine* e : b->eng)
-        if (e->stream) cudaStreamSynchronize(e->stream);
+    drop_graphs(b);
     for (cudaEvent_t ev : b->join) cudaEventDestroy(ev);
     for (cudaEvent_t ev : b->ready) cudaEventDestroy(ev);
     if (b->done) cudaEventDestroy(b->done);

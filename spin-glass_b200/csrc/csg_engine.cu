@@ -592,9 +592,14 @@ void free_engine(csg_engine* e) {
     void* ptrs[] = {e->spins, e->bonds, e->e_sum, e->m_sum, e->q_sum, e->q2_sum, e->q4_sum,
                     e->hist, e->e_last, e->m_last, e->d_last, e->swap_acc, e->swap_log,
                     e->boundary, e->rec_scratch};
-    for (void* p : ptrs)
-        if (p) cudaFree(p);
-    if (e->stream) cudaStreamDestroy(e->stream);
+    for (void* p : ptrs) {
+        if (!p) continue;
+        if (e->pool)
+            cudaFreeAsync(p, e->stream);  // back to the pool after the stream's work
+        else
+            cudaFree(p);
+    }
+    if (e->stream && e->own_stream) cudaStreamDestroy(e->stream);
 }
 
 int reset_obs(csg_engine* e) {
@@ -618,18 +623,22 @@ int reset_obs(csg_engine* e) {
 
 }  // namespace
 
-extern "C" {
-
-const char* csg_last_error(void) { return last_error().c_str(); }
-
-int csg_engine_footprint(const csg_config* cfg, size_t* bytes) {
-    if (int rc = validate(cfg)) return rc;
-    if (!bytes) return fail(CSG_ERR_ARG, "null output");
-    *bytes = footprint_bytes(*cfg);
+int csg_detail::engine_alloc(csg_engine* e, void** p, size_t bytes) {
+    *p = nullptr;
+    if (bytes == 0) return CSG_OK;
+    const cudaError_t ce = e->pool ? cudaMallocFromPoolAsync(p, bytes, e->pool, e->stream)
+                                   : cudaMalloc(p, bytes);
+    if (ce != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return fail(CSG_ERR_NOMEM, std::string(e->pool ? "cudaMallocFromPoolAsync: " : "cudaMalloc: ") +
+                                       cudaGetErrorString(ce));
+    }
     return CSG_OK;
 }
 
-int csg_engine_create(const csg_config* cfg, csg_engine** out) {
+int csg_detail::engine_create_pooled(const csg_config* cfg, cudaMemPool_t pool, cudaStream_t stream,
+                                     csg_engine** out) {
     if (!out) return fail(CSG_ERR_ARG, "null output pointer");
     *out = nullptr;
     if (int rc = validate(cfg)) return rc;
@@ -645,17 +654,21 @@ int csg_engine_create(const csg_config* cfg, csg_engine** out) {
     e->n_e = (size_t)d.n_words * d.n_copies * d.n_temps * 32;
     e->n_q = d.n_copies == 2 ? (size_t)d.n_words * d.n_temps * 32 : 0;
     e->n_hist = d.n_copies == 2 ? (size_t)d.n_temps * (N + 1) : 0;
-    int rc = CSG_OK;
-    // stops at the first failure (nothing more is allocated)
-    auto alloc = [&](auto** p, size_t n) {
-        if (rc == CSG_OK) rc = dalloc(p, n);
-    };
-    if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    if (pool) {
+        e->pool = pool;
+        e->stream = stream;
+        e->own_stream = false;
+    } else if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
         cudaGetLastError();
         e->stream = nullptr;
         delete e;
         return fail(CSG_ERR_CUDA, "cudaStreamCreate failed");
     }
+    int rc = CSG_OK;
+    // stops at the first failure (nothing more is allocated)
+    auto alloc = [&](auto** p, size_t n) {
+        if (rc == CSG_OK) rc = engine_alloc(e, reinterpret_cast<void**>(p), n * sizeof(**p));
+    };
     alloc(&e->spins, e->n_spins);
     alloc(&e->bonds, e->n_bonds);
     alloc(&e->e_sum, e->n_e);
@@ -688,6 +701,27 @@ int csg_engine_create(const csg_config* cfg, csg_engine** out) {
     }
     *out = e;
     return CSG_OK;
+}
+
+void csg_detail::engine_release(csg_engine* e) {
+    if (!e) return;
+    free_engine(e);
+    delete e;
+}
+
+extern "C" {
+
+const char* csg_last_error(void) { return last_error().c_str(); }
+
+int csg_engine_footprint(const csg_config* cfg, size_t* bytes) {
+    if (int rc = validate(cfg)) return rc;
+    if (!bytes) return fail(CSG_ERR_ARG, "null output");
+    *bytes = footprint_bytes(*cfg);
+    return CSG_OK;
+}
+
+int csg_engine_create(const csg_config* cfg, csg_engine** out) {
+    return engine_create_pooled(cfg, nullptr, nullptr, out);
 }
 
 int csg_engine_destroy(csg_engine* e) {
@@ -874,14 +908,8 @@ int csg_obs_records(csg_engine* e, float* rec, size_t n_floats) {
     // scratch: integers, the phase tables, the records
     const size_t o_m = nE * 4, o_d = o_m + nE * 4, o_p = o_d + nD * 4, o_cs = (o_p + nP * 4 + 15) & ~(size_t)15;
     const size_t o_rec = o_cs + (size_t)2 * L * 8, bytes = o_rec + need * 4;
-    if (!e->rec_scratch) {
-        const cudaError_t ce = cudaMalloc(reinterpret_cast<void**>(&e->rec_scratch), bytes);
-        if (ce != cudaSuccess) {
-            cudaGetLastError();
-            e->rec_scratch = nullptr;
-            return fail(CSG_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(ce));
-        }
-    }
+    if (!e->rec_scratch)
+        if (int rc = engine_alloc(e, reinterpret_cast<void**>(&e->rec_scratch), bytes)) return rc;
     char* sc = e->rec_scratch;
     int* de = reinterpret_cast<int*>(sc);
     int* dm = reinterpret_cast<int*>(sc + o_m);

@@ -35,6 +35,12 @@ struct csg_engine {
     int nseg = 0;  // column segments per thread (threads per quad = L * L/2 * nseg)
     // device scratch of csg_obs_records, allocated at its first call
     char* rec_scratch = nullptr;
+    // Set for a server's engines: device memory comes from this pool in the
+    // order of the engine's stream (cudaMallocFromPoolAsync / cudaFreeAsync),
+    // so creating and releasing the engine never waits for the device; the
+    // stream then belongs to the server.
+    cudaMemPool_t pool = nullptr;
+    bool own_stream = true;
 };
 
 #define CSG_INTERNAL __attribute__((visibility("hidden")))
@@ -58,6 +64,16 @@ struct PlanChoice {
 CSG_INTERNAL int fail(int code, const std::string& msg);
 CSG_INTERNAL void set_last_error(const std::string& msg);
 CSG_INTERNAL const std::string& last_error();
+
+// An engine whose device memory comes from `pool` in the order of `stream`
+// (borrowed, not destroyed with the engine), and its release: the memory goes
+// back to the pool in stream order and nothing waits for the device.
+CSG_INTERNAL int engine_create_pooled(const csg_config* cfg, cudaMemPool_t pool,
+                                      cudaStream_t stream, csg_engine** out);
+CSG_INTERNAL void engine_release(csg_engine* e);
+
+// Device memory for an engine: from its pool (stream-ordered) or cudaMalloc.
+CSG_INTERNAL int engine_alloc(csg_engine* e, void** p, size_t bytes);
 
 // Configuration checks.
 CSG_INTERNAL int validate(const csg_config* cfg);

@@ -21,18 +21,83 @@
 
 namespace csg {
 
+// Column sums of the 4 planes of a warp whose 32 lanes all hold counters of
+// one quad: two rounds of lane exchange (lanes i, i^16, then i, i^8) leave
+// each lane with one plane, k = lane >> 3, summed over 4 lanes (two more
+// counter levels); one 32x32 transpose per level then gives every lane j the
+// bits of sample j of all lanes, plane k in bits 8k..8k+7.  Returns, in lane
+// j, the totals of sample j for planes 0..3.
+template <int NLV>
+__device__ __forceinline__ void packed_column_counts(const uint32_t (&v)[4][NLV], int lane,
+                                                     int (&cnt)[4]) {
+    const bool hi16 = (lane & 16) != 0, hi8 = (lane & 8) != 0;
+    uint32_t a[2][NLV + 1];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        uint32_t cy = 0;
+#pragma unroll
+        for (int l = 0; l < NLV; ++l) {
+            const uint32_t mine = hi16 ? v[k + 2][l] : v[k][l];
+            const uint32_t other = __shfl_xor_sync(0xFFFFFFFFu, hi16 ? v[k][l] : v[k + 2][l], 16);
+            a[k][l] = mine ^ other ^ cy;
+            cy = maj3(mine, other, cy);
+        }
+        a[k][NLV] = cy;
+    }
+    uint32_t b[NLV + 2];
+    uint32_t cy = 0;
+#pragma unroll
+    for (int l = 0; l <= NLV; ++l) {
+        const uint32_t mine = hi8 ? a[1][l] : a[0][l];
+        const uint32_t other = __shfl_xor_sync(0xFFFFFFFFu, hi8 ? a[0][l] : a[1][l], 8);
+        b[l] = mine ^ other ^ cy;
+        cy = maj3(mine, other, cy);
+    }
+    b[NLV + 1] = cy;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) cnt[k] = 0;
+#pragma unroll
+    for (int l = 0; l < NLV + 2; ++l) {
+        uint32_t x = b[l];
+#pragma unroll
+        for (int d = 16; d >= 1; d >>= 1) {  // 32x32 bit transpose (as in column_popc)
+            const uint32_t m = d == 16 ? 0x0000FFFFu
+                             : d == 8  ? 0x00FF00FFu
+                             : d == 4  ? 0x0F0F0F0Fu
+                             : d == 2  ? 0x33333333u
+                                       : 0x55555555u;
+            const bool upper = (lane & d) != 0;
+            const uint32_t t = __shfl_xor_sync(0xFFFFFFFFu, x, d);
+            const uint32_t rot = __funnelshift_r(t, t, upper ? d : 32 - d);
+            const uint32_t keep = upper ? ~m : m;
+            x = (x & keep) | (rot & ~keep);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) cnt[k] += __popc((x >> (8 * k)) & 0xFFu) << l;
+    }
+}
+
 // Adds, for each of the 4 planes k of the lane's quad jj, the per-sample
 // column counts of the warp's bit-sliced counters v[k] to dst_of(jj)[32k + b].
-// When a warp holds lanes of two quads (a team size that is not a multiple of
-// 32), each quad's lanes are counted in a pass of their own.  Lanes with
-// jj >= Qc (the CTA's padding threads) hold zeros and count nothing.
+// A warp of one quad reduces all 4 planes in one transpose per level
+// (packed_column_counts); a warp holding lanes of two quads (a team size that
+// is not a multiple of 32) counts each quad's lanes in a pass of their own.
+// Lanes with jj >= Qc (the CTA's padding threads) hold zeros and count nothing.
 template <int NLV, class DstOf>
 __device__ __forceinline__ void add_plane_counts(const uint32_t (&v)[4][NLV], int jj, int Qc,
                                                  int lane, DstOf&& dst_of) {
     const int jlo = __shfl_sync(0xFFFFFFFFu, jj, 0);
     const int jhi = __shfl_sync(0xFFFFFFFFu, jj, 31);
-    const int parts = jlo == jhi ? 1 : 2;
-    for (int part = 0; part < parts; ++part) {
+    if (jlo == jhi) {
+        if (jlo >= Qc) return;  // a warp of padding threads
+        int cnt[4];
+        packed_column_counts<NLV>(v, lane, cnt);
+        int* d = dst_of(jlo);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) atomicAdd(d + k * 32 + lane, cnt[k]);
+        return;
+    }
+    for (int part = 0; part < 2; ++part) {
         const int jp = part ? jhi : jlo;
         if (jp >= Qc) continue;  // uniform over the warp
         const bool mine = jj == jp;
@@ -53,6 +118,24 @@ __device__ __forceinline__ void add_plane_counts(const uint32_t (&v)[4][NLV], in
 #define CSG_UNROLL_ALL_ZS 8
 #endif
 constexpr int kUnrollAllZS = CSG_UNROLL_ALL_ZS;
+// Longer columns run as a loop over groups of sites: the largest even divisor
+// of the column length up to this many.
+#ifndef CSG_SITE_GROUP
+#define CSG_SITE_GROUP 4
+#endif
+// 1: one copy of the colour pass serves both colours, the energy counting
+// guarded by a flag (half the code); 0: a copy with and one without counting.
+#ifndef CSG_RUNTIME_ACC
+#define CSG_RUNTIME_ACC 0
+#endif
+constexpr bool kRuntimeAcc = CSG_RUNTIME_ACC != 0;
+
+__host__ __device__ constexpr int site_group(int zs, int cap) {
+    int u = 2;
+    for (int d = 2; d <= cap && d <= zs; d += 2)
+        if (zs % d == 0) u = d;
+    return u;
+}
 
 template <int L, bool GEN_H, int NSEG>
 __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_constant__ PtParams P) {
@@ -187,9 +270,10 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
 #pragma unroll
             for (int l = 0; l < NLV; ++l) ecnt[k][l] = 0;
 
-        // one colour of the checkerboard; ACC: also add the post-flip
-        // unsatisfied-bond counts into the energy counters
-        auto colour_pass = [&](const int p, auto acc_tag) {
+        // one colour of the checkerboard; ACC (and, with runtime counting,
+        // accum): also add the post-flip unsatisfied-bond counts into the
+        // energy counters
+        auto colour_pass = [&](const int p, auto acc_tag, const bool accum) {
             constexpr bool ACC = decltype(acc_tag)::value;
             // x parity of the column's sites alternates along z: sites k = 0, 2, ...
             // have x = 2h + o0, sites k = 1, 3, ... x = 2h + 1 - o0
@@ -247,20 +331,24 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
                         fl = flip_h0(sa, ca, sb, cb, rr[kq], th0[kq], th1[kq], th2[kq]);
                     cw[kq] = s0 ^ fl;
                     if constexpr (ACC) {
-                        wd[kq][0] = sa ^ fl;
-                        wd[kq][1] = sb ^ fl;
-                        wd[kq][2] = ca ^ fl;
-                        wd[kq][3] = cb ^ fl;
+                        if (accum) {
+                            wd[kq][0] = sa ^ fl;
+                            wd[kq][1] = sb ^ fl;
+                            wd[kq][2] = ca ^ fl;
+                            wd[kq][3] = cb ^ fl;
+                        }
                     }
                 }
                 st4(Sc, off, make_uint4(cw[0], cw[1], cw[2], cw[3]));
             };
             auto acc2 = [&](const uint32_t (&wa)[4][4], const uint32_t (&wb)[4][4]) {
                 if constexpr (ACC) {
+                    if (accum) {
 #pragma unroll
-                    for (int kq = 0; kq < 4; ++kq)
-                        vc_add_2sites<NLV>(ecnt[kq], wa[kq][0], wa[kq][1], wa[kq][2], wa[kq][3],
-                                           wb[kq][0], wb[kq][1], wb[kq][2], wb[kq][3]);
+                        for (int kq = 0; kq < 4; ++kq)
+                            vc_add_2sites<NLV>(ecnt[kq], wa[kq][0], wa[kq][1], wa[kq][2], wa[kq][3],
+                                               wb[kq][0], wb[kq][1], wb[kq][2], wb[kq][3]);
+                    }
                 }
             };
             if constexpr (ZS <= kUnrollAllZS) {
@@ -272,35 +360,46 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
                         site(k + 1, true, -PL, k + 1 == ZS - 1 ? dzL : PL, wb);
                         acc2(wa, wb);
                     } else if constexpr (ACC) {
+                        if (accum) {
 #pragma unroll
-                        for (int kq = 0; kq < 4; ++kq)
-                            vc_add_site<NLV>(ecnt[kq], wa[kq][0], wa[kq][1], wa[kq][2], wa[kq][3]);
+                            for (int kq = 0; kq < 4; ++kq)
+                                vc_add_site<NLV>(ecnt[kq], wa[kq][0], wa[kq][1], wa[kq][2], wa[kq][3]);
+                        }
                     }
                 }
             } else {
-                static_assert(ZS % 2 == 0, "long columns run in pairs of sites");
-                uint32_t wa[4][4], wb[4][4];
-                site(0, false, dzF, PL, wa);
-                site(1, true, -PL, PL, wb);
-                acc2(wa, wb);
+                // groups of U sites: a group's sites sit at fixed offsets from
+                // its first one; only the first group's first site and the last
+                // group's last site wrap around in z
+                constexpr int U = site_group(ZS, CSG_SITE_GROUP);
+                static_assert(ZS % U == 0 && U % 2 == 0, "groups must tile the column");
 #pragma unroll 1
-                for (int k = 2; k < ZS - 2; k += 2) {
-                    site(k, false, -PL, PL, wa);
-                    site(k + 1, true, -PL, PL, wb);
-                    acc2(wa, wb);
+                for (int k0 = 0; k0 < ZS; k0 += U) {
+                    const int dzm0 = k0 == 0 ? dzF : -PL;
+                    const int dzpL = k0 + U == ZS ? dzL : PL;
+#pragma unroll
+                    for (int u = 0; u < U; u += 2) {
+                        uint32_t wa[4][4], wb[4][4];
+                        site(k0 + u, false, u == 0 ? dzm0 : -PL, PL, wa);
+                        site(k0 + u + 1, true, -PL, u + 2 == U ? dzpL : PL, wb);
+                        acc2(wa, wb);
+                    }
                 }
-                site(ZS - 2, false, -PL, PL, wa);
-                site(ZS - 1, true, -PL, dzL, wb);
-                acc2(wa, wb);
             }
         };
-        if (active) colour_pass(0, std::false_type{});
-        __syncthreads();
-        if (active) {
-            if (need_E)
-                colour_pass(1, std::true_type{});
-            else
-                colour_pass(1, std::false_type{});
+        if constexpr (kRuntimeAcc) {
+            if (active) colour_pass(0, std::true_type{}, false);
+            __syncthreads();
+            if (active) colour_pass(1, std::true_type{}, need_E);
+        } else {
+            if (active) colour_pass(0, std::false_type{}, false);
+            __syncthreads();
+            if (active) {
+                if (need_E)
+                    colour_pass(1, std::true_type{}, true);
+                else
+                    colour_pass(1, std::false_type{}, false);
+            }
         }
         __syncthreads();
 
@@ -331,13 +430,9 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
             }
             add_plane_counts<NLD>(mc, jt, Qc, lane, [&](int jj) { return sM + jj * 4 * 32; });
         }
-        __syncthreads();
-        // convert to E_b = 2U - 3N and M = 2 n_up - N
-        for (int i = tid; i < Qc * 4 * 32; i += nthreads) {
-            sE[i] = 2 * sE[i] - 3 * N;
-            if (need_M) sM[i] = 2 * sM[i] - N;
-        }
-
+        // sE / sM hold per-sample counts: U unsatisfied bonds (E_b = 2U - 3N)
+        // and n_up up spins (M = 2 n_up - N); the barriers before their
+        // readers below complete them
         uint32_t mask_keep = 0;  // exchange mask word this thread later finds in sD
         if (do_swap) {
             const long long round = (s + 1) / P.sps - 1;
@@ -380,8 +475,10 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
                         E1 = cluster.map_shared_rank(sE + j2 * 4 * 32, r2);
                         M1 = cluster.map_shared_rank(sM + j2 * 4 * 32, r2);
                     }
-                    const int e0 = E0[lane], e1 = E1[lane];
-                    const int m0 = need_M ? M0[lane] : 0, m1 = need_M ? M1[lane] : 0;
+                    const int u0 = E0[lane], u1 = E1[lane];
+                    const int n0 = need_M ? M0[lane] : 0, n1 = need_M ? M1[lane] : 0;
+                    const int e0 = 2 * u0 - 3 * N, e1 = 2 * u1 - 3 * N;
+                    const int m0 = 2 * n0 - N, m1 = 2 * n1 - N;
                     const double u = pi == warp ? u_first : uniform_for(pi);
                     const double dE = __dsub_rn((double)(e0 - e1), __dmul_rn(P.H, (double)(m0 - m1)));
                     const double delta = __dmul_rn(__dsub_rn(P.tab.beta[t], P.tab.beta[t + 1]), dE);
@@ -393,11 +490,11 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
                     }
                     mask = __ballot_sync(0xFFFFFFFFu, acc);
                     if (acc) {
-                        E0[lane] = e1;
-                        E1[lane] = e0;
+                        E0[lane] = u1;
+                        E1[lane] = u0;
                         if (need_M) {
-                            M0[lane] = m1;
-                            M1[lane] = m0;
+                            M0[lane] = n1;
+                            M1[lane] = n0;
                         }
                     }
                     if (lane == 0) {
@@ -472,13 +569,15 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
                 const int gg = rank * Qc + (pl >> 2);
                 const int cc = gg % C, t = 4 * (gg / C) + (pl & 3);
                 const size_t o = (((size_t)w * C + cc) * T + t) * 32 + b;
+                const int ev = 2 * sE[i] - 3 * N;
                 if (P.e_sum) atomicAdd(reinterpret_cast<unsigned long long*>(P.e_sum + o),
-                                       (unsigned long long)(long long)sE[i]);
-                if (P.e_last) P.e_last[o] = sE[i];
+                                       (unsigned long long)(long long)ev);
+                if (P.e_last) P.e_last[o] = ev;
                 if (need_M) {
+                    const int mv = 2 * sM[i] - N;
                     if (P.m_sum) atomicAdd(reinterpret_cast<unsigned long long*>(P.m_sum + o),
-                                           (unsigned long long)(long long)sM[i]);
-                    if (P.m_last) P.m_last[o] = sM[i];
+                                           (unsigned long long)(long long)mv);
+                    if (P.m_last) P.m_last[o] = mv;
                 }
             }
             if (C == 2) {

@@ -22,6 +22,7 @@ def _run(*args, timeout=600):
 def test_reference_arm_line():
     d = _run("--impl", "reference", "--steps", "1", "--warmup", "1")
     assert d["impl"] == "reference"
+    assert d["config"]["workload"].startswith("batched")
     for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
               "higher_is_better", "config", "cpu_baseline", "e2e"):
         assert k in d, k
@@ -37,9 +38,12 @@ def test_our_arm_line():
     d = _run("--steps", "3", "--warmup", "3", "--no-cpu-baseline")
     for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
               "higher_is_better", "scaling", "vs_baseline", "dtype", "data", "config",
-              "roofline", "e2e", "gpu_launches", "clocks"):
+              "roofline", "e2e", "gpu_launches", "clocks", "plain_value", "batched_over_plain",
+              "every_sweep_schedule", "tuned_plans"):
         assert k in d, k
     r = d["roofline"]
-    assert r["bound"] == "int" and 0 < r["frac"] < 1.2 and r["peak"] > 0
+    assert r["bound"] == "int" and 0 < r["frac"] < 2 and r["peak"] > 0
     assert d["e2e"]["value"] > 0 and d["e2e"]["h2d_bytes_per_step"] > 0
-    assert d["gpu_launches"] == 3 and d["config"]["workload"]
+    assert d["gpu_launches"] == 3 * 6 and d["config"]["workload"].startswith("batched")
+    assert d["config"]["swap_every"] == 16 and d["config"]["measure_every"] == 1024
+    assert d["every_sweep_schedule"]["plain_value"] > 0
