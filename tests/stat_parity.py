@@ -10,11 +10,14 @@ z = (ours - ref) / sqrt(err_ours^2 + err_ref^2).
   python tests/stat_parity.py <out_dir> [n_files] [L:H ...]
 
 Writes <out_dir>/<LL>-<H>-res.dat and <out_dir>/stat_parity.json.  The series
-files are deleted after each reduction (8.8 GB each at 16 files).
+files (8.8 GB each at 16 files) are written under $CSG_STAT_WORK (default:
+<out_dir>) and deleted after each reduction.  Seeds: 20240000 + L at H = 0,
+plus 100 * round(10000 H) at H != 0 (independent disorder per table).
 """
 from __future__ import annotations
 
 import json
+import os
 import pathlib
 import shutil
 import subprocess
@@ -33,7 +36,8 @@ COLS = ["beta", "chi0", "chi0_err", "xi", "xi_err", "e", "e_err", "m", "m_err"]
 
 
 def run_case(out: pathlib.Path, L: int, H: float, n_files: int, seed: int) -> dict:
-    d = out / f"sim-{L:02d}"
+    work = pathlib.Path(os.environ.get("CSG_STAT_WORK", str(out)))
+    d = work / f"sim-{L:02d}-{H:06.4f}"
     d.mkdir(parents=True, exist_ok=True)
     (d / "csg.conf").write_text(f"L = {L}\nseed = {seed}\n")
     t0 = time.time()
@@ -69,7 +73,8 @@ def main() -> None:
                                                              ("16", "0.1875")]
     results = []
     for L, H in cases:
-        results.append(run_case(out, int(L), float(H), n_files, seed=20240000 + int(L)))
+        seed = 20240000 + int(L) + 100 * int(round(10000 * float(H)))
+        results.append(run_case(out, int(L), float(H), n_files, seed=seed))
         (out / "stat_parity.json").write_text(json.dumps(results, indent=1))
         r = results[-1]
         print(r["L"], r["H"], r["wall_s"], {k: (v["max_abs_z"], v["n_abs_z_gt_3"])
