@@ -284,6 +284,11 @@ int csg_batch_set_plan(csg_batch* b, const int32_t* quads_per_cta);
 /* The launch plan member i runs with (after csg_batch_tune: the tuned one). */
 int csg_batch_member_plan(csg_batch* b, int32_t i, csg_plan* out);
 
+/* Fix member i's tile: quads_per_cta and threads_per_quad (0 in either:
+ * automatic; the other fields are ignored), e.g. a plan an earlier
+ * csg_batch_tune chose. */
+int csg_batch_set_member_plan(csg_batch* b, int32_t i, const csg_plan* plan);
+
 /* ---- Serving: continuous batching -------------------------------------------
  * No counterpart in the reference.  Requests (full simulation configurations
  * plus a sweep count) are queued, admitted FIFO while a device-memory budget

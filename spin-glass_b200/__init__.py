@@ -14,12 +14,14 @@ Arrays use the canonical layout of ``include/csg.h``:
 from __future__ import annotations
 
 import ctypes as C
+import os
 import pathlib
 
 import numpy as np
 
 PKG_DIR = pathlib.Path(__file__).resolve().parent
-LIB_PATH = PKG_DIR / "libcsg.so"
+# the library built beside this file, or another build named by $CSG_LIBRARY
+LIB_PATH = pathlib.Path(os.environ.get("CSG_LIBRARY") or PKG_DIR / "libcsg.so")
 
 CSG_MEASURE_M = 1
 CSG_ENGINE_STREAM = 2
@@ -107,6 +109,7 @@ def lib():
             "csg_batch_set_plan": [vp, vp],
             "csg_batch_member_plan": [vp, C.c_int32, C.POINTER(Plan)],
             "csg_batch_launch": [vp, i64, C.c_int32, vp],
+            "csg_batch_set_member_plan": [vp, C.c_int32, C.POINTER(Plan)],
             "csg_engine_footprint": [C.POINTER(Config), C.POINTER(sz)],
             "csg_server_create": [sz, C.c_int32, C.c_int32, C.POINTER(vp)],
             "csg_server_destroy": [vp],
@@ -153,20 +156,22 @@ def make_config(L: int, n_words: int, n_copies: int, betas, *, H: float = 0.0, s
 class Observables:
     """Host copies of the engine's accumulators (shapes as in include/csg.h)."""
 
-    def __init__(self, L: int, W: int, C_: int, T: int, log_rounds: int = 0):
+    def __init__(self, L: int, W: int, C_: int, T: int, log_rounds: int = 0, alloc=np.zeros):
+        """alloc(shape, dtype) makes each array (e.g. in page-locked memory, for
+        faster device-to-host copies when the same object is refilled)."""
         N = L ** 3
         two = C_ == 2
-        self.e_sum = np.zeros((W, C_, T, 32), np.int64)
-        self.m_sum = np.zeros((W, C_, T, 32), np.int64)
-        self.q_sum = np.zeros((W, T, 32) if two else (0,), np.int64)
-        self.q2_sum = np.zeros((W, T, 32) if two else (0,), np.int64)
-        self.q4_sum = np.zeros((W, T, 32, 2) if two else (0,), np.uint64)
-        self.hist = np.zeros((T, N + 1) if two else (0,), np.uint32)
-        self.e_last = np.zeros((W, C_, T, 32), np.int32)
-        self.m_last = np.zeros((W, C_, T, 32), np.int32)
-        self.d_last = np.zeros((W, T, 32) if two else (0,), np.int32)
-        self.swap_acc = np.zeros((C_, T), np.uint64)
-        self.swap_log = np.zeros((max(log_rounds, 1), W, C_, T), np.uint32)
+        self.e_sum = alloc((W, C_, T, 32), np.int64)
+        self.m_sum = alloc((W, C_, T, 32), np.int64)
+        self.q_sum = alloc((W, T, 32) if two else (0,), np.int64)
+        self.q2_sum = alloc((W, T, 32) if two else (0,), np.int64)
+        self.q4_sum = alloc((W, T, 32, 2) if two else (0,), np.uint64)
+        self.hist = alloc((T, N + 1) if two else (0,), np.uint32)
+        self.e_last = alloc((W, C_, T, 32), np.int32)
+        self.m_last = alloc((W, C_, T, 32), np.int32)
+        self.d_last = alloc((W, T, 32) if two else (0,), np.int32)
+        self.swap_acc = alloc((C_, T), np.uint64)
+        self.swap_log = alloc((max(log_rounds, 1), W, C_, T), np.uint32)
         self.c = ObservablesC()
         for f in ("e_sum", "m_sum", "q_sum", "q2_sum", "q4_sum", "hist", "e_last", "m_last",
                   "d_last", "swap_acc", "swap_log"):
@@ -240,10 +245,14 @@ class Engine:
     def run(self, n_sweeps: int) -> None:
         _check(lib().csg_run(self._h, n_sweeps))
 
-    def observables(self) -> Observables:
-        o = Observables(self.L, self.W, self.C, self.T, self._log_rounds)
+    def observables(self, out: Observables | None = None) -> Observables:
+        """The accumulated observables (into `out`, made by new_observables, when given)."""
+        o = out if out is not None else self.new_observables()
         _check(lib().csg_get_observables(self._h, C.byref(o.c)))
         return o
+
+    def new_observables(self, alloc=np.zeros) -> Observables:
+        return Observables(self.L, self.W, self.C, self.T, self._log_rounds, alloc=alloc)
 
     def reset_observables(self) -> None:
         _check(lib().csg_reset_observables(self._h))
@@ -381,6 +390,11 @@ class Batch:
     def set_plan(self, quads_per_cta) -> None:
         q = np.ascontiguousarray(quads_per_cta, np.int32)
         _check(lib().csg_batch_set_plan(self._h, _p(q)))
+
+    def set_member_plan(self, i: int, quads_per_cta: int, threads_per_quad: int = 0) -> None:
+        """Fix member i's tile (0: automatic)."""
+        p = Plan(quads_per_cta, 0, threads_per_quad, 0)
+        _check(lib().csg_batch_set_member_plan(self._h, i, C.byref(p)))
 
     def member_plan(self, i: int) -> "Plan":
         """Launch plan member i runs with (the tuned one after tune())."""

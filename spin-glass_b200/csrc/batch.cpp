@@ -237,6 +237,24 @@ int csg_batch_set_plan(csg_batch* b, const int32_t* quads_per_cta) {
     return CSG_OK;
 }
 
+int csg_batch_set_member_plan(csg_batch* b, int32_t i, const csg_plan* plan) {
+    if (!b || !plan || i < 0 || i >= (int32_t)b->eng.size()) return fail(CSG_ERR_ARG, "bad member index");
+    csg_engine* e = b->eng[i];
+    const int qc = plan->quads_per_cta, tpq = plan->threads_per_quad;
+    if (qc < 0 || tpq < 0) return fail(CSG_ERR_ARG, "negative plan entry");
+    const int L = e->cfg.dims.L;
+    const int nseg = tpq > 0 ? tpq / (L * (L / 2)) : 0;
+    if (tpq > 0 && nseg * L * (L / 2) != tpq) return fail(CSG_ERR_ARG, "threads_per_quad is not L*L/2*s");
+    bool ok = qc == 0 && nseg == 0;
+    for (const PlanChoice& o : plan_options(e->cfg))
+        if ((qc == 0 || o.qc == qc) && (nseg == 0 || o.nseg == nseg)) ok = true;
+    if (!ok) return fail(CSG_ERR_UNSUPPORTED, "no built tile with these quads per CTA and threads per quad");
+    e->qc = qc;
+    e->nseg = nseg;
+    drop_graphs(b);
+    return CSG_OK;
+}
+
 int csg_batch_member_plan(csg_batch* b, int32_t i, csg_plan* out) {
     if (!b || !out || i < 0 || i >= (int32_t)b->eng.size()) return fail(CSG_ERR_ARG, "bad member index");
     Plan pl;

@@ -160,22 +160,30 @@ size_t smem_for(int L, int Qc, bool has_m, bool gen) {
 
 constexpr size_t kMaxSmem = 227 * 1024;
 
+// Shared-memory carve-out (percent) that holds a CTA of smem bytes (plus the
+// 1 KB the system reserves per CTA): the rest of the SM's 256 KB stays L1 for
+// the bonds.
+int carveout_pct(size_t smem) {
+    const int pct = (int)((smem + 1024) * 100 / (228 * 1024));
+    return pct < 100 ? pct : 100;
+}
+
 std::mutex g_plan_mu;
 csg_plan g_override = {0, 0, 0, 0};
 
 int prepare_kernel(KernelFn fn, size_t smem, int K) {
     // the limit covers every plan of this kernel (several engines may share it)
     CSG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
-    // Ask for the smallest shared-memory carve-out that holds the CTA (plus the
-    // 1 KB the system reserves per CTA) so that the rest of the SM's 256 KB
-    // stays L1 for the bonds.
-    const int pct = (int)((smem + 1024) * 100 / (228 * 1024));
+    // the smallest carve-out that holds the CTA (also given per launch)
     CSG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                  pct < 100 ? pct : 100));
+                                  carveout_pct(smem)));
     if (K > 8) CSG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     return CSG_OK;
 }
 
+// attr must hold 2 entries.  The carve-out travels with the launch (and with
+// a graph's kernel node), so plans of other engines that set the kernel's
+// own carve-out attribute do not change it.
 void fill_launch(cudaLaunchConfig_t& lc, cudaLaunchAttribute* attr, int W, const Plan& pl,
                  cudaStream_t st) {
     lc = cudaLaunchConfig_t{};
@@ -187,8 +195,10 @@ void fill_launch(cudaLaunchConfig_t& lc, cudaLaunchAttribute* attr, int W, const
     attr[0].val.clusterDim.x = (unsigned)pl.K;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
+    attr[1].id = cudaLaunchAttributePreferredSharedMemoryCarveout;
+    attr[1].val.sharedMemCarveout = (unsigned)carveout_pct(pl.smem);
     lc.attrs = attr;
-    lc.numAttrs = 1;
+    lc.numAttrs = 2;
 }
 
 // Launch plan: split the G = C*T/4 quads of a word over K = G/Qc CTAs of a
@@ -236,7 +246,7 @@ int make_plan(const csg_config& cfg, bool gen, Plan& out, PlanChoice forced = Pl
             if (pl.K > 16 || pl.smem > kMaxSmem || pl.threads > csg::kMaxThreads) continue;
             if (prepare_kernel(fn, pl.smem, pl.K) != CSG_OK) continue;
             cudaLaunchConfig_t lc;
-            cudaLaunchAttribute attr[1];
+            cudaLaunchAttribute attr[2];
             fill_launch(lc, attr, W, pl, nullptr);
             int nclusters = 0;
             if (cudaOccupancyMaxActiveClusters(&nclusters, fn, &lc) != cudaSuccess || nclusters < 1) {
@@ -502,7 +512,7 @@ int csg_detail::run_device(const csg_config& cfg, uint32_t* spins, const uint32_
         P.sweep0 = sweep0 + done;
         P.n_sweeps = (int)std::min<int64_t>(kSweepsPerLaunch, n_sweeps - done);
         cudaLaunchConfig_t lc;
-        cudaLaunchAttribute attr[1];
+        cudaLaunchAttribute attr[2];
         fill_launch(lc, attr, cfg.dims.n_words, pl, st);
         CSG_CUDA(cudaLaunchKernelEx(&lc, fn, P));
         if (sweep_dev) {

@@ -12,7 +12,8 @@ z = (ours - ref) / sqrt(err_ours^2 + err_ref^2).
 Writes <out_dir>/<LL>-<H>-res.dat and <out_dir>/stat_parity.json.  The series
 files (8.8 GB each at 16 files) are written under $CSG_STAT_WORK (default:
 <out_dir>) and deleted after each reduction.  Seeds: 20240000 + L at H = 0,
-plus 100 * round(10000 H) at H != 0 (independent disorder per table).
+plus 100 * round(10000 H) at H != 0 (independent disorder per table), plus
+$CSG_STAT_SEED_OFFSET (default 0) for a repeat with other disorder.
 """
 from __future__ import annotations
 
@@ -73,7 +74,8 @@ def main() -> None:
                                                              ("16", "0.1875")]
     results = []
     for L, H in cases:
-        seed = 20240000 + int(L) + 100 * int(round(10000 * float(H)))
+        seed = (20240000 + int(L) + 100 * int(round(10000 * float(H))) +
+                int(os.environ.get("CSG_STAT_SEED_OFFSET", "0")))
         results.append(run_case(out, int(L), float(H), n_files, seed=seed))
         (out / "stat_parity.json").write_text(json.dumps(results, indent=1))
         r = results[-1]
