@@ -10,7 +10,16 @@ reference's 9 columns (beta, chi0, err, xi_L/L, err, e, err, m, err) in the
 same format.  Reads the file in chunks, so tables of multi-GB series fit in a
 few hundred MB of memory.
 
-  python spin-glass_b200/analysis.py <obs.bin> <L> <NDIS> <NREP> [SBMEAS] [out.dat]
+Blocked errors (`block` > 1): the reference's errors treat the NDIS samples as
+independent, which they are in its program (every spin of every sample draws
+its own random number).  This engine's draws serve the 32 samples of a word
+(samples 32w .. 32w+31), so their thermal noise is correlated and the
+per-sample variance understates the error where thermal noise dominates the
+disorder spread (the energy at high temperature).  With `block` = 32 the
+errors come from the variance of the word means over the NDIS/32 words, which
+are independent; the means are the same.
+
+  python spin-glass_b200/analysis.py <obs.bin> <L> <NDIS> <NREP> [SBMEAS] [out.dat] [BLOCK]
 """
 from __future__ import annotations
 
@@ -22,8 +31,21 @@ OBS_DT = np.dtype([("e", "f4", (2,)), ("m", "f4", (2,)), ("q_0", "f4"), ("q_1_r"
                    ("q_1_i", "f4", (3,))])
 
 
-def analyze(path: str, L: int, ndis: int, nrep: int, betas=None, chunk: int = 8) -> dict:
-    rec = ndis * nrep * OBS_DT.itemsize
+def _spread(x: np.ndarray, block: int):
+    """Disorder mean, variance and error of per-sample values x[ndis, ...]:
+    the variance over samples (block 1) or over means of `block` consecutive
+    samples, scaled back to one sample (var_block * block), and the error
+    sqrt(var / ndis) of the mean in either case."""
+    if block <= 1:
+        return x.mean(axis=0), x.var(axis=0)
+    xb = x.reshape(x.shape[0] // block, block, *x.shape[1:]).mean(axis=1)
+    return x.mean(axis=0), xb.var(axis=0) * block
+
+
+def analyze(path: str, L: int, ndis: int, nrep: int, betas=None, chunk: int = 8,
+            block: int = 1) -> dict:
+    if block < 1 or ndis % block:
+        raise ValueError("block must divide the number of samples")
     size = np.memmap(path, dtype=np.uint8, mode="r").size
     therm = size // 2
     data = np.memmap(path, dtype=OBS_DT, mode="r", offset=therm)
@@ -44,22 +66,22 @@ def analyze(path: str, L: int, ndis: int, nrep: int, betas=None, chunk: int = 8)
         s_e += d["e"].astype(np.float64).sum(axis=(0, 3))
         s_m += d["m"].astype(np.float64).sum(axis=(0, 3))
     chi0 = s_q0 / n
-    chi0_aa, chi0_v = chi0.mean(axis=0), chi0.var(axis=0)
+    chi0_aa, chi0_v = _spread(chi0, block)
     chi1r, chi1i = s_qr / n, s_qi / n
-    chi1_aa = (chi1r.mean(axis=0) + chi1i.mean(axis=0)).mean(axis=1)
-    chi1_v = (chi1r.var(axis=0) + chi1i.var(axis=0)).mean(axis=1)
+    (r_a, r_v), (i_a, i_v) = _spread(chi1r, block), _spread(chi1i, block)
+    chi1_aa = (r_a + i_a).mean(axis=1)
+    chi1_v = (r_v + i_v).mean(axis=1)
     chif = chi0_aa / chi1_aa
     chif_v = chif ** 2 * (chi0_v / chi0_aa ** 2 + chi1_v / chi1_aa ** 2)
     xi = np.sqrt(chif - 1) / (2 * np.sin(np.pi / L)) / L
     xi_v = (xi / (2 * (chif - 1))) ** 2 * chif_v
-    e = s_e / (2 * n)
-    m = s_m / (2 * n)
+    (e_a, e_v), (m_a, m_v) = _spread(s_e / (2 * n), block), _spread(s_m / (2 * n), block)
     if betas is None:
         betas = np.logspace(1, -3, num=nrep, base=2.0)
     return {"beta": np.asarray(betas), "chi0": chi0_aa, "chi0_err": np.sqrt(chi0_v / ndis),
-            "xi": xi, "xi_err": np.sqrt(xi_v / ndis), "e": e.mean(axis=0),
-            "e_err": np.sqrt(e.var(axis=0) / ndis), "m": m.mean(axis=0),
-            "m_err": np.sqrt(m.var(axis=0) / ndis), "n_meas": n}
+            "xi": xi, "xi_err": np.sqrt(xi_v / ndis), "e": e_a,
+            "e_err": np.sqrt(e_v / ndis), "m": m_a,
+            "m_err": np.sqrt(m_v / ndis), "n_meas": n, "block": block}
 
 
 def analyze_gpu(path: str, L: int, ndis: int, nrep: int, betas=None, device: int = 0) -> dict:
@@ -104,5 +126,6 @@ if __name__ == "__main__":
     obs, L, ndis, nrep = sys.argv[1], int(sys.argv[2]), int(sys.argv[3]), int(sys.argv[4])
     sbmeas = int(sys.argv[5]) if len(sys.argv) > 5 else 1024
     out = sys.argv[6] if len(sys.argv) > 6 else obs.replace("-obs.bin", "-res.dat")
-    write_table(analyze(obs, L, ndis, nrep), out, sbmeas)
+    block = int(sys.argv[7]) if len(sys.argv) > 7 else 1
+    write_table(analyze(obs, L, ndis, nrep, block=block), out, sbmeas)
     print(out)
