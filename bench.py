@@ -145,15 +145,14 @@ def int_peak_ops() -> dict:
             "(spin-glass_b200/csrc/int_peak.cu), best of 5, in this run"}
 
 
-PROFILE_TRAFFIC_SOURCE = ("constant from the committed ncu summary "
-                          "profiles/pt_resident_L16_production.json (dram__bytes_read.sum + "
-                          "dram__bytes_write.sum of one resident-kernel launch of the production "
-                          "shape); not measured in this run")
+def profile_traffic_source(name: str) -> str:
+    return (f"constant from the committed ncu summary profiles/{name}.json "
+            "(dram__bytes_read.sum + dram__bytes_write.sum per launch); not measured in this run")
 
 
-def profile_traffic():
-    """DRAM bytes per launch of the resident kernel from the committed ncu summary."""
-    f = ROOT / "profiles" / "pt_resident_L16_production.json"
+def profile_traffic(name: str = "pt_resident_L16_production"):
+    """DRAM bytes per launch from a committed ncu summary."""
+    f = ROOT / "profiles" / f"{name}.json"
     if not f.exists():
         return None
     try:
@@ -377,8 +376,10 @@ def run_ours(args, rank: int, world: int, dist) -> None:
                          "ops_per_attempt": OPS_PER_WORD_UPDATE / 32, "peak_source": peak["source"]},
             "e2e": {"value": e2e["value"], "unit": METRIC,
                     "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]},
-            # resident kernel: one launch per 1024-sweep step; streaming engine: five per sweep
-            "gpu_launches": args.steps * (args.sweeps_per_step * 5 if args.engine == "stream" else 1),
+            # resident kernel: one launch per 1024-sweep step; streaming engine
+            # at L=16: four per sweep (fused sweep, decisions, exchange with
+            # overlaps, measurement)
+            "gpu_launches": args.steps * (args.sweeps_per_step * 4 if args.engine == "stream" else 1),
             "exchange_boundary_cases": boundary,
             "clocks": clk.summary()}
     if world == 1 and not args.no_cpu_baseline:
@@ -425,6 +426,7 @@ REF_SCHEDULE = (16, 1024)  # the reference program's SBSHFL, SBMEAS (eamsim.cuh:
 # word updates per mixed-workload sweep (32 attempts each)
 MIXED_WORDS_PER_SWEEP = sum(l ** 3 * w * NCOPY * t for l, w, t in MIXED)
 REF_STEP_SWEEPS = 64  # CPU reference arm: sweeps of every member per step (a bounded sample)
+MIXED_PROFILE = "batch_mixed_L12_14_16"  # ncu summary of one graph launch of MIXED
 
 
 def ladder(t: int, lo: float = T_MIN, hi: float = T_MAX) -> np.ndarray:
@@ -519,16 +521,19 @@ def _batch_e2e(torch, b, steps: int) -> dict:
         return [e.observables(out=o) for e, o in zip(b.members, outs)]
 
     step(0)  # untimed: first graph capture for this sweep count
-    t0 = time.perf_counter()
+    marks = [time.perf_counter()]
     for k in range(steps):
         obs = step(k)
-    el = time.perf_counter() - t0
+        marks.append(time.perf_counter())
+    el = marks[-1] - marks[0]
+    per_step = [(b_ - a_) * 1e3 for a_, b_ in zip(marks, marks[1:])]
     d2h = sum(getattr(o, f).nbytes for o in obs
               for f in ("e_sum", "m_sum", "q_sum", "q2_sum", "q4_sum", "hist", "e_last",
                         "m_last", "d_last", "swap_acc")) + 8 * len(obs)
     h2d = sum(hs.nbytes + hb.nbytes for hs, hb in hosts)
     return {"seconds": el, "attempts": steps * SWEEPS_PER_STEP * MIXED_WORDS_PER_SWEEP * 32,
-            "h2d": int(h2d), "d2h": int(d2h)}
+            "h2d": int(h2d), "d2h": int(d2h), "step_ms_median": statistics.median(per_step),
+            "step_ms_max": max(per_step)}
 
 
 def measure_mixed(csg, torch, dev, stream, flush, dist, args, sps, spm, rank, e2e=False,
@@ -671,7 +676,8 @@ def run_mixed(args, rank: int, world: int, dist) -> None:
     roof = int_roofline(words_per_launch, main_m["per_launch_ms"], peak)
     roof.update({"kernel": "the batch graph: the members' pt_resident_kernel launches running "
                            "side by side (one graph launch per step)",
-                 "traffic": profile_traffic(), "traffic_source": PROFILE_TRAFFIC_SOURCE})
+                 "traffic": profile_traffic(MIXED_PROFILE),
+                 "traffic_source": profile_traffic_source(MIXED_PROFILE)})
     line = {"metric": METRIC, "value": head["value"], "unit": METRIC, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
             "sweeps_per_step": SWEEPS_PER_STEP, "higher_is_better": True, "scaling": "weak",
@@ -684,7 +690,9 @@ def run_mixed(args, rank: int, world: int, dist) -> None:
                     "h2d_bytes_per_step": main_m.get("e2e", {}).get("h2d", 0),
                     "d2h_bytes_per_step": main_m.get("e2e", {}).get("d2h", 0),
                     "path": "csg_set_state (pinned host) + csg_batch_run + csg_get_observables "
-                            "(pinned host), every member, every step; wall clock"},
+                            "(pinned host), every member, every step; wall clock",
+                    "step_ms_median": main_m.get("e2e", {}).get("step_ms_median"),
+                    "step_ms_max": main_m.get("e2e", {}).get("step_ms_max")},
             # per step one graph launch: each member's resident kernel and its
             # sweep-counter kernel
             "gpu_launches": args.steps * 2 * len(MIXED),
@@ -724,7 +732,8 @@ def run_large(args) -> None:
     state, 64 MiB of spins, stays in L2).  The roofline line is the colour
     kernel's: its algorithmic bytes per launch (read and write its colour's
     spin words, read the other colour's once, read the bonds once per word)
-    over its event-timed duration in a Metropolis-only run."""
+    over its event-timed duration in a Metropolis-only run.  Each size is
+    measured again with the opt-in fused sweep launch (CSG_STREAM_FUSED)."""
     import torch
     csg = _package()
     dev = torch.device("cuda", 0)
@@ -735,13 +744,15 @@ def run_large(args) -> None:
     by_L = {}
     clk_summary = None
     sizes = [c for c in LARGE if args.large_L in (None, c[0])]
-    for (L_, W_, T_) in sizes:
+    def measure(L_, W_, T_, flags):
+        """One lattice size with the engine's default Metropolis launches
+        (flags 0) or the fused sweep launch (CSG_STREAM_FUSED)."""
         N = L_ ** 3
         betas = 1.0 / (LARGE_T[0] * (LARGE_T[1] / LARGE_T[0]) ** (np.arange(T_) / (T_ - 1)))
         cfg, _k1 = csg.make_config(L_, W_, NCOPY, betas, seed=SEED, sweeps_per_swap=1,
-                                   sweeps_per_meas=1)
+                                   sweeps_per_meas=1, flags=flags)
         metro, _k2 = csg.make_config(L_, W_, NCOPY, betas, seed=SEED, sweeps_per_swap=0,
-                                     sweeps_per_meas=0)
+                                     sweeps_per_meas=0, flags=flags)
         spins = torch.empty(W_ * NCOPY * T_ * N, dtype=torch.int32, device=dev)
         bonds = torch.empty(W_ * 3 * N, dtype=torch.int32, device=dev)
         z64 = lambda *s: torch.zeros(s, dtype=torch.int64, device=dev)
@@ -774,9 +785,10 @@ def run_large(args) -> None:
                 ev[k][1].record(stream)
             torch.cuda.synchronize(dev)
         t_ms = sum(a.elapsed_time(b) for a, b in ev)
-        if L_ == sizes[-1][0]:
-            clk_summary = clk.summary()
-        # colour kernel alone: Metropolis-only sweeps (two colour launches each)
+        # the Metropolis kernel alone: Metropolis-only sweeps (two colour
+        # launches each, or one fused sweep launch)
+        fused = csg.query_plan(L_, W_, NCOPY, betas, flags=flags).smem_bytes > 0
+        per_sweep_launches = 1 if fused else 2
         n_metro = 64
         run(metro, 8, with_obs=False)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -785,25 +797,40 @@ def run_large(args) -> None:
         run(metro, n_metro, with_obs=False)
         b.record(stream)
         torch.cuda.synchronize(dev)
-        colour_s = a.elapsed_time(b) * 1e-3 / (2 * n_metro)
+        colour_s = a.elapsed_time(b) * 1e-3 / (per_sweep_launches * n_metro)
         per_sweep = N * 32 * W_ * NCOPY * T_
-        # per colour launch: half a sweep's attempts; 1.47 int ops and
-        # (8 + 12/(2 n_T))/32 HBM bytes per attempt (one pass per sweep)
-        launch_att = per_sweep / 2
+        # per launch: half a sweep's attempts (colour launch) or a sweep's
+        # (fused); 1.47 int ops and (8 + 12/(2 n_T))/32 HBM bytes per attempt
+        # (one pass per sweep)
+        launch_att = per_sweep / per_sweep_launches
         colour_ops = launch_att * OPS_PER_WORD_UPDATE / 32
         colour_bytes = launch_att * (8 + 12 / (2 * T_)) / 32
-        by_L[L_] = {"attempts_per_ns": args.steps * args.sweeps_per_step * per_sweep / (t_ms * 1e6),
-                    "ms_per_step": t_ms / args.steps,
-                    "us_per_sweep": t_ms * 1e3 / (args.steps * args.sweeps_per_step),
-                    "spin_bytes": W_ * NCOPY * T_ * N * 4,
-                    "metropolis_attempts_per_ns": per_sweep / (2 * colour_s * 1e9),
-                    "colour_kernel": {"us_per_launch": colour_s * 1e6,
-                                      "algorithmic_bytes_per_launch": colour_bytes,
-                                      "achieved_gbs": colour_bytes / colour_s / 1e9,
-                                      "algorithmic_int_ops_per_launch": colour_ops,
-                                      "achieved_int_tops": colour_ops / colour_s / 1e12},
-                    "exchange_boundary_cases": int(acc["boundary"].item())}
+        out = {"attempts_per_ns": args.steps * args.sweeps_per_step * per_sweep / (t_ms * 1e6),
+               "ms_per_step": t_ms / args.steps,
+               "us_per_sweep": t_ms * 1e3 / (args.steps * args.sweeps_per_step),
+               "spin_bytes": W_ * NCOPY * T_ * N * 4,
+               "metropolis_attempts_per_ns": per_sweep / (per_sweep_launches * colour_s * 1e9),
+               "kernel_name": "stream_sweep_kernel" if fused else "stream_colour_kernel",
+               "launches_per_sweep": (4 if fused else 5),
+               "colour_kernel": {"us_per_launch": colour_s * 1e6,
+                                 "algorithmic_bytes_per_launch": colour_bytes,
+                                 "achieved_gbs": colour_bytes / colour_s / 1e9,
+                                 "algorithmic_int_ops_per_launch": colour_ops,
+                                 "achieved_int_tops": colour_ops / colour_s / 1e12},
+               "exchange_boundary_cases": int(acc["boundary"].item())}
         del spins, bonds, acc
+        return out, clk.summary()
+
+    for (L_, W_, T_) in sizes:
+        by_L[L_], clk = measure(L_, W_, T_, 0)
+        if L_ == sizes[-1][0]:
+            clk_summary = clk
+        # the opt-in fused sweep launch beside it (one pass over the state per
+        # sweep: a third of the DRAM traffic, one CTA per temperature quad)
+        by_L[L_]["fused_sweep_launch"] = {
+            k: v for k, v in measure(L_, W_, T_, csg.CSG_STREAM_FUSED)[0].items()
+            if k in ("attempts_per_ns", "us_per_sweep", "metropolis_attempts_per_ns",
+                     "kernel_name", "launches_per_sweep", "colour_kernel")}
     big = by_L[sizes[-1][0]]
     ipeak = int_peak_ops()
     ck = big["colour_kernel"]
@@ -824,14 +851,17 @@ def run_large(args) -> None:
             "roofline": {"bound": "int", "achieved": ck["achieved_int_tops"],
                          "peak": ipeak["ops_per_s"] / 1e12, "unit": "Tops/s (32-bit integer logic)",
                          "frac": ck["achieved_int_tops"] * 1e12 / ipeak["ops_per_s"],
-                         "traffic": None, "kernel": "stream_colour_kernel (Metropolis only)",
+                         "traffic": None,
+                         "kernel": big["kernel_name"] + " (Metropolis-only sweeps)",
                          "peak_source": ipeak["source"],
                          "hbm": {"achieved": ck["achieved_gbs"], "peak": peak["gbs"], "unit": "GB/s",
                                  "frac": ck["achieved_gbs"] / peak["gbs"],
                                  "peak_source": peak["source"]}},
             "by_L": by_L,
-            # per sweep: 2 colour launches, exchange decisions, exchange with overlap, measurement
-            "gpu_launches": args.steps * args.sweeps_per_step * 5, "clocks": clk_summary}
+            # per sweep: the fused sweep launch (or 2 colour launches), exchange
+            # decisions, exchange with overlap, measurement
+            "gpu_launches": args.steps * args.sweeps_per_step * big["launches_per_sweep"],
+            "clocks": clk_summary}
     print(json.dumps(line), flush=True)
 
 

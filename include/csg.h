@@ -55,9 +55,14 @@ typedef struct csg_schedule {
 
 enum {
     CSG_MEASURE_M = 1,   /* also accumulate magnetisations at measurements */
-    CSG_ENGINE_STREAM = 2 /* run the streaming engine (state in global memory, one
-                             launch per colour) even where the cluster-resident
-                             kernel fits; it always runs for L > 24 */
+    CSG_ENGINE_STREAM = 2, /* run the streaming engine (state in global memory, one
+                              launch per colour) even where the cluster-resident
+                              kernel fits; it always runs for L > 24 */
+    CSG_STREAM_FUSED = 4   /* streaming engine, L <= 58: one launch per sweep that
+                              updates both colours in a single pass over the state
+                              (z-planes staged in shared memory by bulk copies): a
+                              third of the DRAM traffic of the colour launches, but
+                              slower on an otherwise idle B200 (one CTA per quad) */
 };
 
 typedef struct csg_config {
@@ -66,7 +71,7 @@ typedef struct csg_config {
     double H;                /* external field, 0 <= H <= 4 (eamsim.cu:520) */
     uint64_t seed;           /* Philox key of the whole simulation */
     const double* betas;     /* n_temps inverse temperatures (host); exchanges pair t, t+1 */
-    int32_t flags;           /* CSG_MEASURE_M | CSG_ENGINE_STREAM */
+    int32_t flags;           /* CSG_MEASURE_M | CSG_ENGINE_STREAM | CSG_STREAM_FUSED */
     int32_t swap_log_rounds; /* keep accepted-exchange masks of this many rounds (tests) */
     int32_t word0;           /* global index of the first sample word (Philox counter word
                                 2): a simulation split into shards of words with matching

@@ -25,6 +25,7 @@ LIB_PATH = pathlib.Path(os.environ.get("CSG_LIBRARY") or PKG_DIR / "libcsg.so")
 
 CSG_MEASURE_M = 1
 CSG_ENGINE_STREAM = 2
+CSG_STREAM_FUSED = 4
 _lib = None
 
 

@@ -27,8 +27,8 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
           "-ffp-contract=off", "-fmad=false", f"-I{ROOT / 'include'}", f"-I{CSRC}"]
 
 OBJ = PKG / "_build"
-LIB_SOURCES = [CSRC / "csg_engine.cu", CSRC / "batch.cpp", CSRC / "server.cpp",
-               CSRC / "obs_noalloc.cu", CSRC / "analysis_kernels.cu"]
+LIB_SOURCES = [CSRC / "csg_engine.cu", CSRC / "stream_sweep.cu", CSRC / "batch.cpp",
+               CSRC / "server.cpp", CSRC / "obs_noalloc.cu", CSRC / "analysis_kernels.cu"]
 RESIDENT_L = [4, 6, 8, 10, 12, 14, 16, 18, 20, 22, 24]  # lattice sides of the resident kernel
 HEADERS = sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + [ROOT / "include" / "csg.h"]
 LIB_DEPS = LIB_SOURCES + [CSRC / "pt_instances.cu"] + HEADERS

@@ -81,6 +81,15 @@ int capture(csg_batch* b, int64_t n_sweeps, bool with_obs, cudaGraphExec_t* out)
         return fail(CSG_ERR_CUDA, std::string("graph capture: ") +
                                       cudaGetErrorString(ce != cudaSuccess ? ce : ce2));
     }
+    // the capture order (largest clusters first) becomes the placement order
+    // even when the graph's launch waits on other streams and every branch
+    // becomes ready at once
+    std::vector<const uint32_t*> starts;
+    for (size_t i : order) starts.push_back(b->eng[i]->spins);
+    if (int rc2 = chain_launch_starts(g, starts)) {
+        cudaGraphDestroy(g);
+        return rc2;
+    }
     const cudaError_t ce3 = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
     if (ce3 != cudaSuccess)

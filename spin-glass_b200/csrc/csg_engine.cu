@@ -212,7 +212,17 @@ int make_plan(const csg_config& cfg, bool gen, Plan& out, PlanChoice forced = Pl
     const int G = cfg.dims.n_copies * cfg.dims.n_temps / 4;
     if (use_stream(cfg)) {  // fixed launch shapes, nothing to plan
         out = Plan{};
-        out.TPQ = csg::kStreamThreads;
+        int nt = 0, smem = 0;
+        if (cfg.flags & CSG_STREAM_FUSED) csg::stream_sweep_shape(L, &nt, &smem);
+        if (nt > 0) {  // fused sweep launch: one CTA per quad, no clusters
+            out.Qc = 1;
+            out.K = G;
+            out.TPQ = nt;
+            out.threads = nt;
+            out.smem = (size_t)smem;
+        } else {  // colour launches
+            out.TPQ = csg::kStreamThreads;
+        }
         return CSG_OK;
     }
     const bool has_m = gen || (cfg.flags & CSG_MEASURE_M);
@@ -304,7 +314,7 @@ constexpr int64_t kSweepsPerLaunch = 1024;
 // ---------------------------------------------------------------------------
 struct StreamLayout {
     int nblk = 0, nblk_plain = 0, nblk2 = 0;
-    size_t u_acc = 0, up_acc = 0, d_acc = 0, energy = 0, magn = 0, masks = 0, bytes = 0;
+    size_t u_acc = 0, up_acc = 0, d_acc = 0, energy = 0, magn = 0, masks = 0, err = 0, bytes = 0;
 };
 
 StreamLayout stream_layout(const csg_config& c) {
@@ -325,6 +335,7 @@ StreamLayout stream_layout(const csg_config& c) {
     s.energy = off, off += up(planes * 32 * 4);
     s.magn = off, off += up(planes * 32 * 4);
     s.masks = off, off += up(planes * 4);
+    s.err = off, off += 256;
     s.bytes = off;
     return s;
 }
@@ -425,6 +436,10 @@ int run_stream(const csg_config& cfg, uint32_t* spins, const uint32_t* bonds,
     S.energy = reinterpret_cast<int*>(base + lay.energy);
     S.magn = reinterpret_cast<int*>(base + lay.magn);
     S.masks = reinterpret_cast<uint32_t*>(base + lay.masks);
+    S.err = reinterpret_cast<int*>(base + lay.err);
+    CSG_CUDA(cudaMemsetAsync(S.err, 0, sizeof(int), st));
+    // one fused launch per sweep where asked for and its ring of z-planes fits
+    const bool fused = (cfg.flags & CSG_STREAM_FUSED) && csg::stream_sweep_fits(d.L);
 
     const long N = (long)d.L * d.L * d.L;
     const unsigned W = (unsigned)d.n_words, C = (unsigned)d.n_copies, Q = (unsigned)S.Q;
@@ -438,8 +453,13 @@ int run_stream(const csg_config& cfg, uint32_t* spins, const uint32_t* bonds,
         const bool do_meas = spm > 0 && (s + 1) % spm == 0 && s >= cfg.sched.meas_start;
         const bool need_E = do_swap || do_meas;
         const bool need_M = need_E && (gen || (do_meas && (cfg.flags & CSG_MEASURE_M)));
-        colour_launch(gen, false, need_M)(S, lay, 0, s, st);
-        colour_launch(gen, need_E, need_M)(S, lay, 1, s, st);
+        if (fused) {
+            ce = csg::launch_stream_sweep(S, s, gen, need_E, need_M, st);
+            if (ce != cudaSuccess) break;
+        } else {
+            colour_launch(gen, false, need_M)(S, lay, 0, s, st);
+            colour_launch(gen, need_E, need_M)(S, lay, 1, s, st);
+        }
         if (need_E) {
             const long long round = do_swap ? (s + 1) / sps - 1 : 0;
             const int par = (int)(round & 1);
@@ -460,9 +480,16 @@ int run_stream(const csg_config& cfg, uint32_t* spins, const uint32_t* bonds,
         }
         ce = cudaGetLastError();
     }
+    // the fused launches report a staging wait that gave up
+    int err = 0;
+    if (ce == cudaSuccess && fused) {
+        ce = cudaMemcpyAsync(&err, S.err, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+    }
     const cudaError_t ce2 = cudaFreeAsync(base, st);
     if (ce != cudaSuccess) return fail(CSG_ERR_CUDA, std::string("stream launch: ") + cudaGetErrorString(ce));
     if (ce2 != cudaSuccess) return fail(CSG_ERR_CUDA, std::string("cudaFreeAsync: ") + cudaGetErrorString(ce2));
+    if (err) return fail(CSG_ERR_CUDA, "streaming engine: a shared-memory staging wait gave up");
     return CSG_OK;
 }
 
@@ -523,6 +550,36 @@ int csg_detail::run_device(const csg_config& cfg, uint32_t* spins, const uint32_
     return CSG_OK;
 }
 
+
+int csg_detail::chain_launch_starts(cudaGraph_t g, const std::vector<const uint32_t*>& spins) {
+    size_t n = 0;
+    CSG_CUDA(cudaGraphGetNodes(g, nullptr, &n));
+    std::vector<cudaGraphNode_t> nodes(n);
+    CSG_CUDA(cudaGraphGetNodes(g, nodes.data(), &n));
+    std::vector<cudaGraphNode_t> first(spins.size(), nullptr);
+    for (cudaGraphNode_t node : nodes) {
+        cudaGraphNodeType type;
+        CSG_CUDA(cudaGraphNodeGetType(node, &type));
+        if (type != cudaGraphNodeTypeKernel) continue;
+        cudaKernelNodeParams kp = {};
+        CSG_CUDA(cudaGraphKernelNodeGetParams(node, &kp));
+        // every kernel of a captured run_device but the sweep counter's takes PtParams
+        if (kp.func == reinterpret_cast<void*>(csg::advance_counter) || !kp.kernelParams) continue;
+        const csg::PtParams* P = static_cast<const csg::PtParams*>(kp.kernelParams[0]);
+        if (P->sweep0 != 0) continue;  // a later launch of a section longer than one launch
+        for (size_t i = 0; i < spins.size(); ++i)
+            if (P->spins == spins[i]) first[i] = node;
+    }
+    for (size_t i = 1; i < first.size(); ++i) {
+        if (!first[i - 1] || !first[i]) return fail(CSG_ERR_STATE, "captured launch not found");
+        cudaGraphEdgeData ed = {};
+        ed.from_port = cudaGraphKernelNodePortLaunchCompletion;
+        ed.to_port = 0;
+        ed.type = cudaGraphDependencyTypeProgrammatic;
+        CSG_CUDA(cudaGraphAddDependencies_v2(g, &first[i - 1], &first[i], &ed, 1));
+    }
+    return CSG_OK;
+}
 
 std::vector<PlanChoice> csg_detail::plan_options(const csg_config& c) {
     std::vector<PlanChoice> out;

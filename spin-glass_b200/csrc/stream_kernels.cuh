@@ -1,8 +1,10 @@
 // stream_kernels.cuh — parallel tempering for lattices whose temperature quads
 // do not fit in shared memory (L > 24), streamed through L2/HBM.
 //
-// One sweep = two colour launches (stream_colour_kernel), then, when the
-// schedule asks for it, the exchange decisions (stream_decide_kernel), the
+// One sweep = one fused launch that updates both colours in a single pass
+// over the state (stream_sweep.cu, while its ring of z-planes fits in shared
+// memory: L <= 58) or two colour launches (stream_colour_kernel), then, when
+// the schedule asks for it, the exchange decisions (stream_decide_kernel), the
 // masked exchange and the overlap counts in one pass
 // (stream_exchange_overlap_kernel; stream_exchange_kernel or
 // stream_overlap_kernel when only one of them is due) and the measurement
@@ -16,83 +18,9 @@
 #include <cstdint>
 #include <type_traits>
 
-#include "philox.cuh"
-#include "pt_kernel.cuh"
+#include "stream_params.cuh"
 
 namespace csg {
-
-// Launch shapes (measured at L=32 and L=48).  Plain colour launches: blocks of
-// kStreamThreads threads, kStreamSPT sites of the colour per thread.
-constexpr int kStreamThreads = 256;
-constexpr int kStreamSPT = 8;
-// Colour launches that count (energies, magnetisations) run smaller blocks of
-// kStreamAccSitesPerBlock sites (their counters live in shared memory, one
-// column per thread).
-constexpr int kStreamAccThreads = 128;
-constexpr int kStreamAccSPT = 8;
-constexpr int kStreamAccSitesPerBlock = kStreamAccThreads * kStreamAccSPT;
-template <bool ACC>
-__host__ __device__ constexpr int colour_threads() { return ACC ? kStreamAccThreads : kStreamThreads; }
-template <bool ACC>
-__host__ __device__ constexpr int colour_spt() { return ACC ? kStreamAccSPT : kStreamSPT; }
-constexpr int kStreamNLV = bit_length(6 * kStreamAccSPT);  // bits of a per-thread bond count
-constexpr int kStreamNLM = bit_length(kStreamAccSPT);      // bits of a per-thread site count
-// Overlap passes (both copies of every quad): blocks of kStreamThreads threads
-// over kOverlapSitesPerBlock sites (all N sites of a lattice).
-constexpr int kOverlapSPT = 8;
-constexpr int kOverlapSitesPerBlock = kStreamThreads * kOverlapSPT;
-constexpr int kOverlapNL = bit_length(kOverlapSPT);
-
-struct StreamParams {
-    uint32_t* spins;
-    const uint32_t* bonds;
-    // per-plane totals, added to by the blocks (integer atomics: any order gives
-    // the same sums) and cleared by the kernel that consumes them
-    int* u_acc;   // [W][C][T][32] unsatisfied bonds after the sweep
-    int* up_acc;  // [W][C][T][32] spins up after the sweep
-    int* d_acc;   // [W][T][32] sites where the copies differ
-    int* energy;  // [W][C][T][32] bond energies after the exchange
-    int* magn;    // [W][C][T][32]
-    uint32_t* masks;  // [W][C][T] accepted-sample masks of the current round
-    int L, W, C, T, Q;
-    int nblk;   // blocks per quad of a counting colour launch
-    int nblk2;  // blocks per quad of an overlap pass (over all N sites)
-    uint32_t k0, k1, word0;
-    uint32_t mag_plane;  // ceil(2^32 / (L*L/2)): division by multiply-high
-    uint32_t mag_row;    // ceil(2^32 / (L/2))
-    double H;
-    PtTables tab;
-};
-
-// n / d for 0 <= n < L^3/2, d in {L/2, L*L/2}, with mag = ceil(2^32 / d): the
-// multiply-high estimate is never below n / d and at most one above it for
-// every even L <= 128 (checked exhaustively), so one correction makes it exact.
-__device__ __forceinline__ int div_magic(int n, int d, uint32_t mag) {
-    const int q = (int)__umulhi((uint32_t)n, mag);
-    return q - (q * d > n ? 1 : 0);
-}
-
-// Measurement accumulators (layouts as in PtParams / csg_device_obs).
-struct StreamObs {
-    long long* e_sum;
-    long long* m_sum;
-    long long* q_sum;
-    long long* q2_sum;
-    unsigned long long* q4_sum;
-    unsigned int* hist;
-    int* e_last;
-    int* m_last;
-    int* d_last;
-};
-
-// Programmatic dependent launch (the sweep's kernels are launched with it): a
-// kernel waits here until the previous kernel on the stream has finished and
-// its writes are visible, then lets the next kernel's blocks be scheduled as
-// soon as all of its own blocks run, so launch latency overlaps the tail.
-__device__ __forceinline__ void pdl_enter() {
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
 
 // One colour of one sweep.  blockIdx.x = quad (w, c, q), blockIdx.y = block
 // of colour_spt * blockDim.x sites of that colour; each thread updates

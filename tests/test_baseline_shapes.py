@@ -48,6 +48,7 @@ def _oracle(orc, L, W, T, betas, n, H=0.0):
 @pytest.mark.parametrize("L,W,T,trange,n,flags", [
     (16, 32, 24, (0.2, 2.0), 8, 0),   # production
     (48, 8, 32, (0.5, 2.0), 2, 0),    # large lattice (streaming engine)
+    (48, 8, 32, (0.5, 2.0), 2, 4),    # the same, fused sweep launch (CSG_STREAM_FUSED)
 ])
 def test_plain_engine_at_benchmark_shape(csg, orc, L, W, T, trange, n, flags):
     betas = orc.geometric_betas(T, *trange)

@@ -7,7 +7,22 @@ import pytest
 
 def test_large_lattice_plan_and_footprint(csg):
     betas = np.linspace(2.0, 0.5, 8)
+    # colour launches by default
     p = csg.query_plan(32, 2, 2, betas)
+    assert (p.quads_per_cta, p.ctas_per_word, p.threads_per_quad, p.smem_bytes) == (0, 0, 256, 0)
+    # the fused sweep launch (L <= 58) when asked for: one CTA of L*L/2 /
+    # sites-per-thread threads per quad, a ring of 2 x 4 half z-planes (L*L/2 x
+    # 16 bytes each)
+    F = csg.CSG_STREAM_FUSED
+    p = csg.query_plan(32, 2, 2, betas, flags=F)
+    assert (p.quads_per_cta, p.ctas_per_word, p.threads_per_quad, p.smem_bytes) == \
+        (1, 4, 512, 8 * 512 * 16)
+    p = csg.query_plan(48, 1, 2, betas, flags=F)
+    assert (p.threads_per_quad, p.smem_bytes) == (384, 8 * 1152 * 16)
+    p = csg.query_plan(58, 1, 2, betas, flags=F)
+    assert (p.threads_per_quad, p.smem_bytes) == (448, 8 * 1682 * 16)
+    # colour launches beyond it
+    p = csg.query_plan(60, 1, 2, betas, flags=F)
     assert (p.quads_per_cta, p.ctas_per_word, p.threads_per_quad, p.smem_bytes) == (0, 0, 256, 0)
     N = 32 ** 3
     spins = 2 * 2 * 8 * N * 4
@@ -15,6 +30,8 @@ def test_large_lattice_plan_and_footprint(csg):
     # the forced streaming engine plans the same way at small L
     p = csg.query_plan(8, 1, 2, betas, flags=csg.CSG_ENGINE_STREAM)
     assert (p.quads_per_cta, p.threads_per_quad) == (0, 256)
+    p = csg.query_plan(8, 1, 2, betas, flags=csg.CSG_ENGINE_STREAM | F)
+    assert (p.quads_per_cta, p.threads_per_quad, p.smem_bytes) == (1, 32, 8 * 32 * 16)
     assert csg.footprint(8, 1, 2, betas, flags=csg.CSG_ENGINE_STREAM) > \
         csg.footprint(8, 1, 2, betas)
 
@@ -56,18 +73,45 @@ STREAM_CASES = [
     (16, 1, 1, 24, 0.0, 10, 3, 2, 0, True),
     (26, 1, 2, 64, 0.0, 3, 1, 1, 0, False),   # the largest ladder
     (34, 1, 2, 4, 1.1, 3, 1, 1, 0, False),
+    (4, 1, 2, 8, 0.0, 12, 1, 1, 0, True),     # the smallest lattice
+]
+
+# The fused sweep launch (CSG_STREAM_FUSED): its edges (the smallest lattice,
+# one warp per CTA; the largest; three and four sites per thread), the general
+# field, magnetisations, sparse schedules and one copy.
+FUSED_CASES = [
+    (26, 1, 2, 12, 0.0, 6, 1, 1, 0, False),
+    (32, 1, 1, 8, 0.0, 4, 2, 1, 0, False),
+    (30, 1, 2, 8, 0.7, 5, 1, 1, 0, False),
+    (48, 1, 2, 4, 0.0, 3, 1, 1, 0, False),
+    (58, 1, 2, 4, 0.0, 2, 1, 1, 0, False),    # the largest lattice of the fused sweep launch
+    (60, 1, 1, 4, 0.0, 2, 1, 1, 0, False),    # beyond it: colour launches
+    (40, 1, 2, 8, 0.9, 3, 1, 1, 0, False),    # general field, two sites per thread
+    (8, 2, 2, 12, 0.0, 20, 1, 1, 0, True),
+    (4, 1, 2, 8, 0.0, 12, 1, 1, 0, True),     # the smallest lattice: a CTA of one warp
+    (12, 1, 2, 8, 1.3, 16, 2, 1, 3, True),
 ]
 
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("L,W,C_,T,H,n,sps,spm,ms,forced", STREAM_CASES)
 def test_stream_engine_matches_oracle(csg, orc, L, W, C_, T, H, n, sps, spm, ms, forced):
+    _check_stream_case(csg, orc, L, W, C_, T, H, n, sps, spm, ms, forced, 0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("L,W,C_,T,H,n,sps,spm,ms,forced", FUSED_CASES)
+def test_stream_fused_matches_oracle(csg, orc, L, W, C_, T, H, n, sps, spm, ms, forced):
+    _check_stream_case(csg, orc, L, W, C_, T, H, n, sps, spm, ms, forced, csg.CSG_STREAM_FUSED)
+
+
+def _check_stream_case(csg, orc, L, W, C_, T, H, n, sps, spm, ms, forced, extra_flags):
     _gpu()
     seed = 2000 + L * 5 + T
     betas = orc.geometric_betas(T, 0.4, 2.5)
     spins, bonds = orc.init(L, W, C_, T, seed)
     rounds = n // sps if sps else 0
-    flags = csg.CSG_MEASURE_M | (csg.CSG_ENGINE_STREAM if forced else 0)
+    flags = csg.CSG_MEASURE_M | (csg.CSG_ENGINE_STREAM if forced else 0) | extra_flags
     with csg.Engine(L, W, C_, betas, H=H, seed=seed, sweeps_per_swap=sps, sweeps_per_meas=spm,
                     meas_start=ms, flags=flags, swap_log_rounds=max(rounds, 1)) as e:
         e.set_state(spins, bonds, 0)
