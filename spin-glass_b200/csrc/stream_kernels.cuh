@@ -43,6 +43,8 @@ __global__ void __launch_bounds__(colour_threads<ACC_E || ACC_M>()) stream_colou
     const uint32_t* Fo = Fw + (1 - p) * NH;
     const uint32_t ctr3 = kTagSweep | ((uint32_t)c << 8) | (uint32_t)q;
     const uint32_t wg = (uint32_t)w + P.word0;
+    // the Philox rounds that do not depend on the site, once per launch
+    const PhiloxFixed pf = philox_fix((uint32_t)s, wg, ctr3, P.k0, P.k1);
     const int lane = threadIdx.x & 31;
     uint32_t th0[4], th1[4], th2[4];
 #pragma unroll
@@ -88,8 +90,7 @@ __global__ void __launch_bounds__(colour_threads<ACC_E || ACC_M>()) stream_colou
         const uint32_t f0 = __ldg(Fo + nxm), f1 = __ldg(Fc + n);
         const uint32_t f2 = __ldg(Fo + N + nym), f3 = __ldg(Fc + N + n);
         const uint32_t f4 = __ldg(Fo + 2 * N + nzm), f5 = __ldg(Fc + 2 * N + n);
-        const u32x4 r = philox4x32_10((uint32_t)((z * L + y) * L + x), (uint32_t)s, wg, ctr3,
-                                      P.k0, P.k1);
+        const u32x4 r = philox_c0((uint32_t)((z * L + y) * L + x), pf);
         const uint32_t rr[4] = {r.v0, r.v1, r.v2, r.v3};
         uint32_t cw[4] = {cv.x, cv.y, cv.z, cv.w};
         const uint32_t n0w[4] = {a0.x, a0.y, a0.z, a0.w}, n1w[4] = {a1.x, a1.y, a1.z, a1.w};

@@ -24,6 +24,8 @@
 // CPU oracle.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "pt_resident.cuh"
 #include "stream_params.cuh"
 
@@ -379,11 +381,17 @@ cudaError_t launch_one(const StreamParams& P, long long s, cudaStream_t st) {
     lc.blockDim = dim3((unsigned)nt);
     lc.dynamicSmemBytes = (size_t)smem;
     lc.stream = st;
-    cudaLaunchAttribute a[1];
+    // the smallest shared-memory carve-out that holds the ring (plus the
+    // static part and the 1 KB per-CTA reserve): the rest of the SM's 256 KB
+    // stays L1 for the bonds, each of which is read in two consecutive steps
+    cudaLaunchAttribute a[2];
     a[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     a[0].val.programmaticStreamSerializationAllowed = 1;
+    a[1].id = cudaLaunchAttributePreferredSharedMemoryCarveout;
+    a[1].val.sharedMemCarveout =
+        (unsigned)std::min<size_t>(100, ((size_t)smem + 4096) * 100 / (228 * 1024) + 1);
     lc.attrs = a;
-    lc.numAttrs = 1;
+    lc.numAttrs = 2;
     return cudaLaunchKernelEx(&lc, kernel, P, s);
 }
 
