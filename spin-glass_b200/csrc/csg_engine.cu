@@ -536,7 +536,9 @@ int csg_detail::run_device(const csg_config& cfg, uint32_t* spins, const uint32_
     P.K = pl.K;
     P.Qc = pl.Qc;
     for (int64_t done = 0; done < n_sweeps; done += kSweepsPerLaunch) {
-        P.sweep0 = sweep0 + done;
+        // with a device counter the launches of a section read their start
+        // from it (advanced after each launch); otherwise from the offset
+        P.sweep0 = sweep_dev ? sweep0 : sweep0 + done;
         P.n_sweeps = (int)std::min<int64_t>(kSweepsPerLaunch, n_sweeps - done);
         cudaLaunchConfig_t lc;
         cudaLaunchAttribute attr[2];
@@ -565,8 +567,12 @@ int csg_detail::chain_launch_starts(cudaGraph_t g, const std::vector<const uint3
         CSG_CUDA(cudaGraphKernelNodeGetParams(node, &kp));
         // every kernel of a captured run_device but the sweep counter's takes PtParams
         if (kp.func == reinterpret_cast<void*>(csg::advance_counter) || !kp.kernelParams) continue;
+        // a section's first launch is its branch's root; later launches of a
+        // section longer than one launch follow the sweep counter's kernel
+        size_t n_deps = 0;
+        CSG_CUDA(cudaGraphNodeGetDependencies(node, nullptr, &n_deps));
+        if (n_deps != 0) continue;
         const csg::PtParams* P = static_cast<const csg::PtParams*>(kp.kernelParams[0]);
-        if (P->sweep0 != 0) continue;  // a later launch of a section longer than one launch
         for (size_t i = 0; i < spins.size(); ++i)
             if (P->spins == spins[i]) first[i] = node;
     }

@@ -80,3 +80,27 @@ def test_tuner_keeps_states_and_results(csg, orc):
         b.run(10)
         for m, e in zip(ms, b.members):
             np.testing.assert_array_equal(e.get_state()[0], oracle_state(orc, m, 10)[0])
+
+
+def test_graph_on_caller_stream_after_state_copies(csg, orc):
+    """The graph's members start in capture order through launch-completion
+    edges between their first launches: launched on a fresh caller stream right
+    behind csg_set_state copies, with two members of the same L (told apart by
+    their state buffers) and sections longer than one launch, every member is
+    still bit-equal to the oracle."""
+    import torch
+    ms = members(orc) + [dict(L=8, n_words=1, n_copies=2, betas=orc.geometric_betas(12, 0.5, 2.0),
+                              seed=14, sweeps_per_swap=1, sweeps_per_meas=1)]
+    side = torch.cuda.Stream()
+    n = 1100  # two launches per member: the edges join the first ones only
+    with csg.Batch(ms) as b:
+        for m, e in zip(ms, b.members):
+            T = len(m["betas"])
+            s0, b0 = orc.init(m["L"], m["n_words"], m["n_copies"], T, m["seed"])
+            e.set_state(s0, b0, 0)
+        b.launch(n, side.cuda_stream)
+        side.synchronize()
+        for m, e in zip(ms, b.members):
+            s, _, sweep = e.get_state()
+            assert sweep == n
+            np.testing.assert_array_equal(s, oracle_state(orc, m, n)[0])
