@@ -2,6 +2,8 @@
 for a few sweeps each (the oracle runs a production sweep in tens of ms on a
 host's cores):
 
+* the small plain run: L=12, 32 samples, 2 copies, 16 temperatures in
+  [0.5, 2], its whole 2048 sweeps, exchange and measurement every sweep;
 * production: L=16, 1024 samples (32 words), 2 copies, 24 temperatures
   geometric in T in [0.2, 2], exchange and measurement every sweep;
 * batched, uneven sizes: L=12 x 512 samples (16 T), L=14 x 384 (20 T),
@@ -46,6 +48,7 @@ def _oracle(orc, L, W, T, betas, n, H=0.0):
 
 
 @pytest.mark.parametrize("L,W,T,trange,n,flags", [
+    (12, 1, 16, (0.5, 2.0), 2048, 0),  # the small plain run, whole length (1024 + 1024 sweeps)
     (16, 32, 24, (0.2, 2.0), 8, 0),   # production
     (48, 8, 32, (0.5, 2.0), 2, 0),    # large lattice (streaming engine)
     (48, 8, 32, (0.5, 2.0), 2, 4),    # the same, fused sweep launch (CSG_STREAM_FUSED)
