@@ -21,62 +21,6 @@
 
 namespace csg {
 
-// Column sums of the 4 planes of a warp whose 32 lanes all hold counters of
-// one quad: two rounds of lane exchange (lanes i, i^16, then i, i^8) leave
-// each lane with one plane, k = lane >> 3, summed over 4 lanes (two more
-// counter levels); one 32x32 transpose per level then gives every lane j the
-// bits of sample j of all lanes, plane k in bits 8k..8k+7.  Returns, in lane
-// j, the totals of sample j for planes 0..3.
-template <int NLV>
-__device__ __forceinline__ void packed_column_counts(const uint32_t (&v)[4][NLV], int lane,
-                                                     int (&cnt)[4]) {
-    const bool hi16 = (lane & 16) != 0, hi8 = (lane & 8) != 0;
-    uint32_t a[2][NLV + 1];
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-        uint32_t cy = 0;
-#pragma unroll
-        for (int l = 0; l < NLV; ++l) {
-            const uint32_t mine = hi16 ? v[k + 2][l] : v[k][l];
-            const uint32_t other = __shfl_xor_sync(0xFFFFFFFFu, hi16 ? v[k][l] : v[k + 2][l], 16);
-            a[k][l] = mine ^ other ^ cy;
-            cy = maj3(mine, other, cy);
-        }
-        a[k][NLV] = cy;
-    }
-    uint32_t b[NLV + 2];
-    uint32_t cy = 0;
-#pragma unroll
-    for (int l = 0; l <= NLV; ++l) {
-        const uint32_t mine = hi8 ? a[1][l] : a[0][l];
-        const uint32_t other = __shfl_xor_sync(0xFFFFFFFFu, hi8 ? a[0][l] : a[1][l], 8);
-        b[l] = mine ^ other ^ cy;
-        cy = maj3(mine, other, cy);
-    }
-    b[NLV + 1] = cy;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) cnt[k] = 0;
-#pragma unroll
-    for (int l = 0; l < NLV + 2; ++l) {
-        uint32_t x = b[l];
-#pragma unroll
-        for (int d = 16; d >= 1; d >>= 1) {  // 32x32 bit transpose (as in column_popc)
-            const uint32_t m = d == 16 ? 0x0000FFFFu
-                             : d == 8  ? 0x00FF00FFu
-                             : d == 4  ? 0x0F0F0F0Fu
-                             : d == 2  ? 0x33333333u
-                                       : 0x55555555u;
-            const bool upper = (lane & d) != 0;
-            const uint32_t t = __shfl_xor_sync(0xFFFFFFFFu, x, d);
-            const uint32_t rot = __funnelshift_r(t, t, upper ? d : 32 - d);
-            const uint32_t keep = upper ? ~m : m;
-            x = (x & keep) | (rot & ~keep);
-        }
-#pragma unroll
-        for (int k = 0; k < 4; ++k) cnt[k] += __popc((x >> (8 * k)) & 0xFFu) << l;
-    }
-}
-
 // Adds, for each of the 4 planes k of the lane's quad jj, the per-sample
 // column counts of the warp's bit-sliced counters v[k] to dst_of(jj)[32k + b].
 // A warp of one quad reduces all 4 planes in one transpose per level

@@ -166,10 +166,19 @@ __global__ void __launch_bounds__(colour_threads<ACC_E || ACC_M>()) stream_colou
         }
         for (int i = threadIdx.x; i < 2 * 4 * 32; i += BT) (&sred[0][0][0])[i] = 0;
         __syncthreads();
+        // all lanes of a block hold counters of its one quad: the 4 planes of a
+        // warp in one 32x32 transpose per counter level
+        if constexpr (ACC_E) {
+            int cnt[4];
+            packed_column_counts<NLV>(ecnt, lane, cnt);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            if constexpr (ACC_E) atomicAdd(&sred[0][k][lane], column_count<NLV>(ecnt[k], lane));
-            if constexpr (ACC_M) atomicAdd(&sred[1][k][lane], column_count<NLM>(mcnt[k], lane));
+            for (int k = 0; k < 4; ++k) atomicAdd(&sred[0][k][lane], cnt[k]);
+        }
+        if constexpr (ACC_M) {
+            int cnt[4];
+            packed_column_counts<NLM>(mcnt, lane, cnt);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) atomicAdd(&sred[1][k][lane], cnt[k]);
         }
         __syncthreads();
         if (threadIdx.x < 128) {

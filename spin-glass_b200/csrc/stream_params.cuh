@@ -20,7 +20,10 @@ constexpr int kStreamSPT = 8;
 // kStreamAccSitesPerBlock sites (their counters live in shared memory, one
 // column per thread).
 constexpr int kStreamAccThreads = 128;
-constexpr int kStreamAccSPT = 8;
+#ifndef CSG_STREAM_ACC_SPT
+#define CSG_STREAM_ACC_SPT 8
+#endif
+constexpr int kStreamAccSPT = CSG_STREAM_ACC_SPT;
 constexpr int kStreamAccSitesPerBlock = kStreamAccThreads * kStreamAccSPT;
 template <bool ACC>
 __host__ __device__ constexpr int colour_threads() { return ACC ? kStreamAccThreads : kStreamThreads; }
