@@ -25,7 +25,8 @@ namespace csg {
 // column counts of the warp's bit-sliced counters v[k] to dst_of(jj)[32k + b].
 // A warp of one quad reduces all 4 planes in one transpose per level
 // (packed_column_counts); a warp holding lanes of two quads (a team size that
-// is not a multiple of 32) counts each quad's lanes in a pass of their own.
+// is not a multiple of 32) does so once per quad, the other quad's lanes
+// counting zeros.
 // Lanes with jj >= Qc (the CTA's padding threads) hold zeros and count nothing.
 template <int NLV, class DstOf>
 __device__ __forceinline__ void add_plane_counts(const uint32_t (&v)[4][NLV], int jj, int Qc,
@@ -45,14 +46,17 @@ __device__ __forceinline__ void add_plane_counts(const uint32_t (&v)[4][NLV], in
         const int jp = part ? jhi : jlo;
         if (jp >= Qc) continue;  // uniform over the warp
         const bool mine = jj == jp;
+        // the other quad's lanes count as zeros
+        uint32_t x[4][NLV];
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+#pragma unroll
+            for (int l = 0; l < NLV; ++l) x[k][l] = mine ? v[k][l] : 0u;
+        int cnt[4];
+        packed_column_counts<NLV>(x, lane, cnt);
         int* d = dst_of(jp);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            uint32_t x[NLV];
-#pragma unroll
-            for (int l = 0; l < NLV; ++l) x[l] = mine ? v[k][l] : 0u;
-            atomicAdd(d + k * 32 + lane, column_count<NLV>(x, lane));
-        }
+        for (int k = 0; k < 4; ++k) atomicAdd(d + k * 32 + lane, cnt[k]);
     }
 }
 
