@@ -637,12 +637,27 @@ def measure_production(csg, torch, dev, stream, flush, args) -> dict:
         lambda k: csg.run_device(cfg, spins.data_ptr(), bonds.data_ptr(), obs,
                                  SWEEP0 + k * SWEEPS_PER_STEP, SWEEPS_PER_STEP, stream.cuda_stream))
     att = args.steps * SWEEPS_PER_STEP * attempts_per_sweep()
-    return {"config": workload_config(1), "value": att / (t_ms * 1e6),
-            "ms_per_step": t_ms / args.steps,
-            "roofline": int_roofline(SWEEPS_PER_STEP * W * NCOPY * T * N, per, int_peak_ops()),
-            "plan": {"quads_per_cta": plan.quads_per_cta, "ctas_per_word": plan.ctas_per_word,
-                     "threads_per_quad": plan.threads_per_quad},
-            "exchange_boundary_cases": int(acc["boundary"].item())}
+    peak = int_peak_ops()
+    out = {"config": workload_config(1), "value": att / (t_ms * 1e6),
+           "ms_per_step": t_ms / args.steps,
+           "roofline": int_roofline(SWEEPS_PER_STEP * W * NCOPY * T * N, per, peak),
+           "plan": {"quads_per_cta": plan.quads_per_cta, "ctas_per_word": plan.ctas_per_word,
+                    "threads_per_quad": plan.threads_per_quad},
+           "exchange_boundary_cases": int(acc["boundary"].item())}
+    # the same shape with the exchange every sweep but the measurement at the
+    # reference program's cadence (every 1024 sweeps): what the per-sweep
+    # measurement costs
+    cfg2, _keep2 = csg.make_config(L, W, NCOPY, betas, seed=SEED, sweeps_per_swap=1,
+                                   sweeps_per_meas=REF_SCHEDULE[1])
+    t2, per2 = _time_launches(
+        torch, dev, stream, flush, None, args.steps, args.warmup,
+        lambda k: csg.run_device(cfg2, spins.data_ptr(), bonds.data_ptr(), obs,
+                                 SWEEP0 + k * SWEEPS_PER_STEP, SWEEPS_PER_STEP, stream.cuda_stream))
+    out["measure_every_1024"] = {"value": att / (t2 * 1e6), "ms_per_step": t2 / args.steps,
+                                 "roofline_frac": int_roofline(SWEEPS_PER_STEP * W * NCOPY * T * N,
+                                                               per2, peak)["frac"],
+                                 "schedule": "exchange every sweep, measurement every 1024"}
+    return out
 
 
 def run_mixed(args, rank: int, world: int, dist) -> None:
