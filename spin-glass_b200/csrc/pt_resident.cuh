@@ -362,18 +362,14 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
 #pragma unroll
                 for (int l = 0; l < NLD; ++l) mc[k][l] = 0;
             if (active) {
+                // four consecutive sites of a plane per 128-bit load
 #pragma unroll 1
-                for (int n = lt; n < N; n += 4 * TPQ) {
-                    uint4 v[4];
+                for (int i = lt; i < N / 4; i += TPQ) {
 #pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        const int nn = n + u * TPQ;
-                        v[u] = nn < N ? ld4(Sq, nn) : make_uint4(0, 0, 0, 0);
+                    for (int k = 0; k < 4; ++k) {
+                        const uint4 v = reinterpret_cast<const uint4*>(Sq + k * N)[i];
+                        vc_add4<NLD>(mc[k], v.x, v.y, v.z, v.w);
                     }
-                    vc_add4<NLD>(mc[0], v[0].x, v[1].x, v[2].x, v[3].x);
-                    vc_add4<NLD>(mc[1], v[0].y, v[1].y, v[2].y, v[3].y);
-                    vc_add4<NLD>(mc[2], v[0].z, v[1].z, v[2].z, v[3].z);
-                    vc_add4<NLD>(mc[3], v[0].w, v[1].w, v[2].w, v[3].w);
                 }
             }
             add_plane_counts<NLD>(mc, jt, Qc, lane, [&](int jj) { return sM + jj * 4 * 32; });
@@ -468,23 +464,35 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
             // exchange the masked bits of two planes, chunks of 8 sites: all
             // loads (some perhaps from a peer CTA) are in flight before the
             // first store
+            // four consecutive sites of a plane per 128-bit access (N is a
+            // multiple of 8, the plane arrays 16-byte aligned)
             auto exchange = [&](uint32_t* pa, uint32_t* pb, const uint32_t m) {
-                constexpr int CH = 8;
-                for (int n0 = lt; n0 < N; n0 += CH * TPQ) {
-                    uint32_t a[CH], b[CH];
+                constexpr int N4 = N / 4, CH = 2;
+                uint4* const a4 = reinterpret_cast<uint4*>(pa);
+                uint4* const b4 = reinterpret_cast<uint4*>(pb);
+                auto mix = [m](uint32_t& x, uint32_t& y) {
+                    const uint32_t d = (x ^ y) & m;
+                    x ^= d;
+                    y ^= d;
+                };
+                for (int i0 = lt; i0 < N4; i0 += CH * TPQ) {
+                    uint4 a[CH], b[CH];
 #pragma unroll
                     for (int u = 0; u < CH; ++u) {
-                        const int n = n0 + u * TPQ;
-                        a[u] = n < N ? pa[n] : 0u;
-                        b[u] = n < N ? pb[n] : 0u;
+                        const int i = i0 + u * TPQ;
+                        a[u] = i < N4 ? a4[i] : make_uint4(0, 0, 0, 0);
+                        b[u] = i < N4 ? b4[i] : make_uint4(0, 0, 0, 0);
                     }
 #pragma unroll
                     for (int u = 0; u < CH; ++u) {
-                        const int n = n0 + u * TPQ;
-                        if (n < N) {
-                            const uint32_t d = (a[u] ^ b[u]) & m;
-                            pa[n] = a[u] ^ d;
-                            pb[n] = b[u] ^ d;
+                        const int i = i0 + u * TPQ;
+                        if (i < N4) {
+                            mix(a[u].x, b[u].x);
+                            mix(a[u].y, b[u].y);
+                            mix(a[u].z, b[u].z);
+                            mix(a[u].w, b[u].w);
+                            a4[i] = a[u];
+                            b4[i] = b[u];
                         }
                     }
                 }
@@ -545,23 +553,15 @@ __global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_c
 #pragma unroll
                     for (int l = 0; l < NLH; ++l) dc[k][l] = 0;
                 if (active) {
+                    // four consecutive sites of a plane per 128-bit load
 #pragma unroll 2
-                    for (int n = lt; n < NH; n += 4 * TPQ) {
-                        uint4 v[4];
+                    for (int i = lt; i < NH / 4; i += TPQ) {
 #pragma unroll
-                        for (int u = 0; u < 4; ++u) {
-                            const int nn = n + u * TPQ;
-                            if (nn < NH) {
-                                const uint4 a = ld4(Sh, nn), b = ld4(Sp, nn);
-                                v[u] = make_uint4(a.x ^ b.x, a.y ^ b.y, a.z ^ b.z, a.w ^ b.w);
-                            } else {
-                                v[u] = make_uint4(0, 0, 0, 0);
-                            }
+                        for (int k = 0; k < 4; ++k) {
+                            const uint4 a = reinterpret_cast<const uint4*>(Sh + k * N)[i];
+                            const uint4 b = reinterpret_cast<const uint4*>(Sp + k * N)[i];
+                            vc_add4<NLH>(dc[k], a.x ^ b.x, a.y ^ b.y, a.z ^ b.z, a.w ^ b.w);
                         }
-                        vc_add4<NLH>(dc[0], v[0].x, v[1].x, v[2].x, v[3].x);
-                        vc_add4<NLH>(dc[1], v[0].y, v[1].y, v[2].y, v[3].y);
-                        vc_add4<NLH>(dc[2], v[0].z, v[1].z, v[2].z, v[3].z);
-                        vc_add4<NLH>(dc[3], v[0].w, v[1].w, v[2].w, v[3].w);
                     }
                 }
                 // counts of quad jj go to the copy-0 quad of its temperature quad
