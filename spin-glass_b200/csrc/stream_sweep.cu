@@ -9,12 +9,11 @@
 // updates colour 0 in plane z, then (after a barrier) colour 1 in plane z-1:
 //   colour 0 at z   reads colour 1 at z-1, z, z+1 as they were before the sweep;
 //   colour 1 at z-1 reads colour 0 at z-2, z-1, z, all updated by then.
-// A plane's bonds are read in two consecutive steps, so their second reads
-// hit L1 (the ring leaves ~90 KB of it at L = 48).  Colour 1 of plane 0 waits
-// until the end (it needs colour 0 of plane L-1), and the
-// planes past L-1 (colour 1 of plane 0 before its update, colour 0 of planes
-// 0 and 1 after theirs) are read back from global memory, where each update
-// is written as soon as it is made.  New colour-0 words also go to their ring
+// A plane's bonds are read in two consecutive steps (the ring leaves ~90 KB
+// of L1 at L = 48 for them).  Colour 1 of plane 0 waits until the end (it
+// needs colour 0 of plane L-1), and the planes past L-1 (colour 1 of plane 0
+// before its update, colour 0 of planes 0 and 1 after theirs) are read back
+// from global memory, where each update is written as soon as it is made.  New colour-0 words also go to their ring
 // slot (colour 1 reads them there); new colour-1 words only to global memory.
 // Every word of the state is read once and written once per sweep.
 //
