@@ -370,7 +370,8 @@ __global__ void __launch_bounds__(kSweepMaxThreads) stream_sweep_kernel(const __
 template <bool G, bool E, bool M, int SPT>
 cudaError_t launch_one(const StreamParams& P, long long s, cudaStream_t st) {
     auto* kernel = stream_sweep_kernel<G, E, M, SPT>;
-    static const cudaError_t attr = cudaFuncSetAttribute(
+    // set on every launch: the attribute belongs to the current device
+    const cudaError_t attr = cudaFuncSetAttribute(
         kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSweepMaxSmem);
     if (attr != cudaSuccess) return attr;
     int nt = 0, smem = 0;
