@@ -277,10 +277,11 @@ int csg_batch_launch(csg_batch* b, int64_t n_sweeps, int32_t plain, void* stream
 
 /* Autotuner: chooses each member's tile — quads per CTA (hence its cluster
  * size) and threads per quad (how many z-segments a column of the checkerboard
- * is split into) — and whether every member CTA gets an SM of its own, by
- * timing the whole batch graph for probe_sweeps sweeps; states are restored
- * after.  chosen (may be NULL) receives the quads per CTA per member;
- * csg_batch_member_plan reports the whole plan. */
+ * is split into) — and, per member, whether each of its CTAs gets an SM of
+ * its own (its shared memory padded past half an SM), by timing the whole
+ * batch graph for probe_sweeps sweeps; states are restored after.  chosen
+ * (may be NULL) receives the quads per CTA per member; csg_batch_member_plan
+ * reports the whole plan (smem_bytes includes the padding). */
 int csg_batch_tune(csg_batch* b, int64_t probe_sweeps, int32_t* chosen);
 
 /* Set each member's quads per CTA (0 = automatic; threads per quad automatic). */

@@ -26,9 +26,9 @@ struct csg_batch {
     cudaEvent_t done = nullptr;
     long long* counters = nullptr;  // device sweep counter per member
     std::vector<std::pair<int64_t, cudaGraphExec_t>> graphs;
-    // pad every member CTA's shared memory past half an SM, so that no two
-    // CTAs share an SM (chosen by the tuner)
-    bool spread = false;
+    // per member: pad its CTAs' shared memory past half an SM, so that none
+    // of them shares an SM (chosen by the tuner)
+    std::vector<char> spread;
 };
 
 namespace {
@@ -44,7 +44,7 @@ constexpr size_t kSpreadSmem = 116 * 1024;
 int capture(csg_batch* b, int64_t n_sweeps, bool with_obs, cudaGraphExec_t* out) {
     std::vector<Plan> plans(b->eng.size());
     for (size_t i = 0; i < b->eng.size(); ++i)
-        if (int rc = plan_engine(b->eng[i], plans[i], b->spread ? kSpreadSmem : 0)) return rc;
+        if (int rc = plan_engine(b->eng[i], plans[i], b->spread[i] ? kSpreadSmem : 0)) return rc;
     // Branches in order of decreasing cluster size (then shared memory per CTA):
     // the GPU places the clusters of the first branches first, and putting the
     // largest first packs the GPCs best (best-fit decreasing).  On the mixed
@@ -152,7 +152,10 @@ int csg_batch_create(const csg_config* cfgs, int32_t n, csg_batch** out) {
             rc = fail(CSG_ERR_UNSUPPORTED,
                       "batch members need the cluster-resident kernel (L <= 24, no CSG_ENGINE_STREAM)");
         }
-        if (rc == CSG_OK) b->eng.push_back(e);
+        if (rc == CSG_OK) {
+            b->eng.push_back(e);
+            b->spread.push_back(0);
+        }
     }
     if (rc == CSG_OK && cudaStreamCreateWithFlags(&b->main, cudaStreamNonBlocking) != cudaSuccess)
         rc = fail(CSG_ERR_CUDA, "cudaStreamCreate failed");
@@ -267,7 +270,7 @@ int csg_batch_set_member_plan(csg_batch* b, int32_t i, const csg_plan* plan) {
 int csg_batch_member_plan(csg_batch* b, int32_t i, csg_plan* out) {
     if (!b || !out || i < 0 || i >= (int32_t)b->eng.size()) return fail(CSG_ERR_ARG, "bad member index");
     Plan pl;
-    if (int rc = plan_engine(b->eng[i], pl, b->spread ? kSpreadSmem : 0)) return rc;
+    if (int rc = plan_engine(b->eng[i], pl, b->spread[i] ? kSpreadSmem : 0)) return rc;
     out->quads_per_cta = pl.Qc;
     out->ctas_per_word = pl.K;
     out->threads_per_quad = pl.TPQ;
@@ -276,10 +279,10 @@ int csg_batch_member_plan(csg_batch* b, int32_t i, csg_plan* out) {
 }
 
 // Autotuner: times the whole batch graph for probe_sweeps sweeps (best of two)
-// for every combination of the members' quads per CTA, each with and without
-// one SM per CTA, when there are at most 256 such combinations; otherwise
-// coordinate descent over one member at a time
-// with the others fixed (two passes).  The members' spins are saved before and restored
+// for every combination of the members' tiles (quads per CTA, threads per
+// quad), each member with and without an SM per CTA, when there are at most
+// 1024 such combinations; otherwise coordinate descent over one member at a
+// time with the others fixed (two passes).  The members' spins are saved before and restored
 // after, and the probes accumulate no observables, so tuning leaves the
 // simulations exactly as they were.
 int csg_batch_tune(csg_batch* b, int64_t probe_sweeps, int32_t* chosen) {
@@ -341,21 +344,24 @@ int csg_batch_tune(csg_batch* b, int64_t probe_sweeps, int32_t* chosen) {
         b->eng[i]->nseg = pc.nseg;
     };
     auto choice_of = [&](size_t i) { return PlanChoice{b->eng[i]->qc, b->eng[i]->nseg}; };
-    if (2 * combos <= 256) {
-        // few enough combinations: time every one, with and without one SM per
-        // CTA (members share the GPU, so the best plan of one member depends
-        // on the others')
+    // every (plan, spread) combination of every member when there are at most
+    // kMaxProbes of them: members share the GPU, so the best plan of one
+    // member depends on the others'
+    constexpr size_t kMaxProbes = 1024;
+    const size_t masks = n < 16 ? (size_t)1 << n : kMaxProbes + 1;
+    if (combos * masks <= kMaxProbes) {
         float best_ms = 1e30f;
-        bool best_spread = false;
         std::vector<PlanChoice> best(n);
+        std::vector<char> best_spread(b->spread);
         for (size_t i = 0; i < n; ++i) best[i] = choice_of(i);
-        for (size_t k = 0; k < 2 * combos && rc == CSG_OK; ++k) {
-            b->spread = k >= combos;
+        for (size_t k = 0; k < combos * masks && rc == CSG_OK; ++k) {
+            const size_t mask = k / combos;
             size_t r = k % combos;
             for (size_t i = 0; i < n; ++i) {
                 const size_t m = options[i].size();
                 if (m) set_choice(i, options[i][r % m]);
                 r /= std::max<size_t>(1, m);
+                b->spread[i] = (char)((mask >> i) & 1);
             }
             float ms = 0.f;
             if (time_batch(ms) != CSG_OK) {  // e.g. a cluster shape the device cannot place
@@ -371,24 +377,31 @@ int csg_batch_tune(csg_batch* b, int64_t probe_sweeps, int32_t* chosen) {
         for (size_t i = 0; i < n; ++i) set_choice(i, best[i]);
         b->spread = best_spread;
     }
-    for (int pass = 0; pass < 2 && rc == CSG_OK && 2 * combos > 256; ++pass)
+    // otherwise coordinate descent: each member's (plan, spread) in turn with
+    // the others fixed, two passes
+    for (int pass = 0; pass < 2 && rc == CSG_OK && combos * masks > kMaxProbes; ++pass)
         for (size_t i = 0; i < n && rc == CSG_OK; ++i) {
             PlanChoice best_pc = choice_of(i);
+            char best_sp = b->spread[i];
             float best_ms = 1e30f;
-            for (const PlanChoice& pc : options[i]) {
-                set_choice(i, pc);
-                float ms = 0.f;
-                const int r = time_batch(ms);
-                if (r != CSG_OK) {  // e.g. a cluster shape the device cannot place
-                    cudaGetLastError();
-                    continue;
+            for (const PlanChoice& pc : options[i])
+                for (char sp = 0; sp < 2; ++sp) {
+                    set_choice(i, pc);
+                    b->spread[i] = sp;
+                    float ms = 0.f;
+                    const int r = time_batch(ms);
+                    if (r != CSG_OK) {  // e.g. a cluster shape the device cannot place
+                        cudaGetLastError();
+                        continue;
+                    }
+                    if (ms < best_ms) {
+                        best_ms = ms;
+                        best_pc = pc;
+                        best_sp = sp;
+                    }
                 }
-                if (ms < best_ms) {
-                    best_ms = ms;
-                    best_pc = pc;
-                }
-            }
             set_choice(i, best_pc);
+            b->spread[i] = best_sp;
         }
     for (size_t i = 0; i < n; ++i) {
         if (saved[i]) {
