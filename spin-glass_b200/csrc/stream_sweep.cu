@@ -13,8 +13,9 @@
 // of L1 at L = 48 for them).  Colour 1 of plane 0 waits until the end (it
 // needs colour 0 of plane L-1), and the planes past L-1 (colour 1 of plane 0
 // before its update, colour 0 of planes 0 and 1 after theirs) are read back
-// from global memory, where each update is written as soon as it is made.  New colour-0 words also go to their ring
-// slot (colour 1 reads them there); new colour-1 words only to global memory.
+// from global memory, where each update is written as soon as it is made.
+// New colour-0 words also go to their ring slot (colour 1 reads them there);
+// new colour-1 words only to global memory.
 // Every word of the state is read once and written once per sweep.
 //
 // The arithmetic of a site update, the Philox counters and the energy and
