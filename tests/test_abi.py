@@ -75,3 +75,16 @@ def test_missing_library_fails_loudly(csg, monkeypatch, tmp_path):
     monkeypatch.setattr(csg, "LIB_PATH", tmp_path / "nope.so")
     with pytest.raises(RuntimeError, match="missing"):
         csg.lib()
+
+
+def test_flag_constants_match_header(tmp_path, csg):
+    src = tmp_path / "fl.c"
+    src.write_text(
+        '#include <stdio.h>\n#include "csg.h"\n'
+        'int main(void){printf("%d %d %d\\n", CSG_MEASURE_M, CSG_ENGINE_STREAM, '
+        'CSG_STREAM_FUSED); return 0;}\n')
+    exe = tmp_path / "fl"
+    subprocess.run(["gcc", f"-I{ROOT / 'include'}", str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True,
+                                          check=True).stdout.split()]
+    assert got == [csg.CSG_MEASURE_M, csg.CSG_ENGINE_STREAM, csg.CSG_STREAM_FUSED]
