@@ -84,9 +84,13 @@ int capture(csg_batch* b, int64_t n_sweeps, bool with_obs, cudaGraphExec_t* out)
     // the capture order (largest clusters first) becomes the placement order
     // even when the graph's launch waits on other streams and every branch
     // becomes ready at once
-    std::vector<const uint32_t*> starts;
-    for (size_t i : order) starts.push_back(b->eng[i]->spins);
-    if (int rc2 = chain_launch_starts(g, starts)) {
+    std::vector<const csg_engine*> starts;
+    std::vector<int> nsegs;
+    for (size_t i : order) {
+        starts.push_back(b->eng[i]);
+        nsegs.push_back(plans[i].NSEG);
+    }
+    if (int rc2 = chain_launch_starts(g, starts, nsegs)) {
         cudaGraphDestroy(g);
         return rc2;
     }

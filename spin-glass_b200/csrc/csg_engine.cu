@@ -553,28 +553,38 @@ int csg_detail::run_device(const csg_config& cfg, uint32_t* spins, const uint32_
 }
 
 
-int csg_detail::chain_launch_starts(cudaGraph_t g, const std::vector<const uint32_t*>& spins) {
+int csg_detail::chain_launch_starts(cudaGraph_t g, const std::vector<const csg_engine*>& members,
+                                    const std::vector<int>& nseg) {
+    // each member's resident kernel: a node is one of its launches when it
+    // runs that kernel on the member's state buffer
+    std::vector<const void*> fns(members.size());
+    for (size_t i = 0; i < members.size(); ++i) {
+        csg::PtParams P;
+        bool gen = false;
+        fill_params(members[i]->cfg, P, gen);
+        fns[i] = reinterpret_cast<const void*>(select_kernel(members[i]->cfg.dims.L, gen, nseg[i]));
+    }
     size_t n = 0;
     CSG_CUDA(cudaGraphGetNodes(g, nullptr, &n));
     std::vector<cudaGraphNode_t> nodes(n);
     CSG_CUDA(cudaGraphGetNodes(g, nodes.data(), &n));
-    std::vector<cudaGraphNode_t> first(spins.size(), nullptr);
+    std::vector<cudaGraphNode_t> first(members.size(), nullptr);
     for (cudaGraphNode_t node : nodes) {
         cudaGraphNodeType type;
         CSG_CUDA(cudaGraphNodeGetType(node, &type));
         if (type != cudaGraphNodeTypeKernel) continue;
-        cudaKernelNodeParams kp = {};
-        CSG_CUDA(cudaGraphKernelNodeGetParams(node, &kp));
-        // every kernel of a captured run_device but the sweep counter's takes PtParams
-        if (kp.func == reinterpret_cast<void*>(csg::advance_counter) || !kp.kernelParams) continue;
         // a section's first launch is its branch's root; later launches of a
         // section longer than one launch follow the sweep counter's kernel
         size_t n_deps = 0;
         CSG_CUDA(cudaGraphNodeGetDependencies(node, nullptr, &n_deps));
         if (n_deps != 0) continue;
-        const csg::PtParams* P = static_cast<const csg::PtParams*>(kp.kernelParams[0]);
-        for (size_t i = 0; i < spins.size(); ++i)
-            if (P->spins == spins[i]) first[i] = node;
+        cudaKernelNodeParams kp = {};
+        CSG_CUDA(cudaGraphKernelNodeGetParams(node, &kp));
+        for (size_t i = 0; i < members.size(); ++i) {
+            if (kp.func != fns[i] || !kp.kernelParams) continue;
+            const csg::PtParams* P = static_cast<const csg::PtParams*>(kp.kernelParams[0]);
+            if (P->spins == members[i]->spins) first[i] = node;
+        }
     }
     for (size_t i = 1; i < first.size(); ++i) {
         if (!first[i - 1] || !first[i]) return fail(CSG_ERR_STATE, "captured launch not found");

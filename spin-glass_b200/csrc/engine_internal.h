@@ -99,13 +99,15 @@ CSG_INTERNAL int run_device(const csg_config& cfg, uint32_t* spins, const uint32
 
 CSG_INTERNAL csg_device_obs device_obs(const csg_engine* e);
 
-// In a graph captured from run_device calls on several state buffers (spins,
-// in the order given), makes the first resident-kernel launch of each buffer
-// after the first depend on every block of the previous one's first launch
-// having begun (a programmatic edge from its launch-completion port): the
-// GPU then places the launches' clusters in this order however the graph's
-// launch is gated, and nothing waits for a launch to finish.
-CSG_INTERNAL int chain_launch_starts(cudaGraph_t g, const std::vector<const uint32_t*>& spins);
+// In a graph captured from run_device calls of several engines (in the order
+// given, each with the column split nseg of its plan), makes the first
+// resident-kernel launch of each engine after the first depend on every block
+// of the previous one's first launch having begun (a programmatic edge from
+// its launch-completion port): the GPU then places the launches' clusters in
+// this order however the graph's launch is gated, and nothing waits for a
+// launch to finish.
+CSG_INTERNAL int chain_launch_starts(cudaGraph_t g, const std::vector<const csg_engine*>& members,
+                                     const std::vector<int>& nseg);
 
 // Host counters after n sweeps ran: sweep index, exchange rounds, measurements.
 CSG_INTERNAL void account(csg_engine* e, int64_t n);
