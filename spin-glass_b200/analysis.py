@@ -73,7 +73,10 @@ def analyze(path: str, L: int, ndis: int, nrep: int, betas=None, chunk: int = 8,
     chi1_v = (r_v + i_v).mean(axis=1)
     chif = chi0_aa / chi1_aa
     chif_v = chif ** 2 * (chi0_v / chi0_aa ** 2 + chi1_v / chi1_aa ** 2)
-    xi = np.sqrt(chif - 1) / (2 * np.sin(np.pi / L)) / L
+    # chif < 1 (hot temperatures, few measurements) gives NaN, as the
+    # reference's table does; no warning for that expected case
+    with np.errstate(invalid="ignore"):
+        xi = np.sqrt(chif - 1) / (2 * np.sin(np.pi / L)) / L
     xi_v = (xi / (2 * (chif - 1))) ** 2 * chif_v
     (e_a, e_v), (m_a, m_v) = _spread(s_e / (2 * n), block), _spread(s_m / (2 * n), block)
     if betas is None:
