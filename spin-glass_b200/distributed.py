@@ -5,8 +5,10 @@ simulation of W sample words splits into contiguous word ranges, one per rank.
 Each rank runs its range as an ordinary engine whose ``word0`` is the range's
 first global word, which keeps every Philox counter equal to the unsplit
 run's: the union of the shards is bit-identical to running all words on one
-GPU.  The only communication is the final gather of the (small) observable
-accumulators to rank 0 over the process group (NCCL on GPUs, gloo on CPUs).
+GPU.  The only communication is gathers to rank 0 over the process group (NCCL
+on GPUs, gloo on CPUs): the observable accumulators, the reference-format
+records after a section, and the reference-format checkpoint.  csg_sharded.py
+builds the reference program's command on these.
 """
 from __future__ import annotations
 
@@ -37,6 +39,7 @@ class ShardedEngine:
         self.group = group
         self.world = dist.get_world_size(group)
         self.rank = dist.get_rank(group)
+        self.n_words = n_words
         self.word_first, self.n_local = shard(n_words, self.world, self.rank)
         if engine_factory is None:
             from . import Engine as engine_factory  # noqa: N813
@@ -72,3 +75,32 @@ class ShardedEngine:
         out.update(n_meas=parts[0]["n_meas"], swap_rounds=parts[0]["swap_rounds"],
                    boundary=sum(p["boundary"] for p in parts))
         return out
+
+    def gather_records(self):
+        """The obs_s records of every sample on rank 0 (None on other ranks):
+        float32 [32 W][T][11] in sample order, the block the reference program
+        appends to <H>-obs.bin after each section (eamsim.cu:704-708)."""
+        return self.gather_rows(self.engine.obs_records())
+
+    def gather_checkpoint(self):
+        """The reference checkpoint of the whole simulation on rank 0 (None on
+        other ranks): uint32 [64 W][N], lattice 2*sample+copy (eamsim.cu:655-676)."""
+        return self.gather_rows(self.engine.save_checkpoint())
+
+    def load_checkpoint(self, ref, sweep: int = 0) -> None:
+        """Load this rank's rows of a whole-simulation reference checkpoint."""
+        ref = np.asarray(ref)
+        if ref.ndim != 2 or ref.shape[0] != 64 * self.n_words:
+            raise ValueError("checkpoint rows do not match the simulation's samples")
+        rows = ref[64 * self.word_first:64 * (self.word_first + self.n_local)]
+        self.engine.load_checkpoint(np.ascontiguousarray(rows, np.uint32), sweep)
+
+    def gather_rows(self, mine):
+        """This rank's array, whose rows follow its sample words, stacked with
+        the other ranks' on rank 0 in word order (None on other ranks)."""
+        parts = [None] * self.world if self.rank == 0 else None
+        dist.gather_object((self.word_first, mine), parts, dst=0, group=self.group)
+        if self.rank != 0:
+            return None
+        parts.sort(key=lambda p: p[0])
+        return np.concatenate([p[1] for p in parts], axis=0)
