@@ -253,7 +253,8 @@ int make_plan(const csg_config& cfg, bool gen, Plan& out, PlanChoice forced = Pl
             pl.TPQ = csg::threads_per_quad(L, nseg);
             pl.threads = (Qc * pl.TPQ + 31) / 32 * 32;
             pl.smem = smem_for(L, Qc, has_m, gen);
-            if (pl.K > 16 || pl.smem > kMaxSmem || pl.threads > csg::kMaxThreads) continue;
+            if (pl.K > 16 || pl.smem > kMaxSmem || pl.threads > csg::max_cta_threads(gen, nseg))
+                continue;
             if (prepare_kernel(fn, pl.smem, pl.K) != CSG_OK) continue;
             cudaLaunchConfig_t lc;
             cudaLaunchAttribute attr[2];
@@ -610,7 +611,7 @@ std::vector<PlanChoice> csg_detail::plan_options(const csg_config& c) {
         const int tpq = csg::threads_per_quad(L, nseg);
         for (int qc = 1; qc <= G; ++qc)
             if (G % qc == 0 && G / qc <= 16 && smem_for(L, qc, has_m, gen) <= kMaxSmem &&
-                (qc * tpq + 31) / 32 * 32 <= csg::kMaxThreads)
+                (qc * tpq + 31) / 32 * 32 <= csg::max_cta_threads(gen, nseg))
                 out.push_back(PlanChoice{qc, nseg});
     }
     return out;

@@ -23,6 +23,14 @@ namespace cgx = cooperative_groups;
 
 constexpr int kMaxT = 64;
 constexpr int kMaxThreads = 512;  // CTA size cap: keeps 128 registers per thread available
+// The general-field kernels whose threads each walk a whole column (one
+// segment) keep more state live per site than 128 registers hold (they spilled
+// up to 316 bytes at L = 24); their CTAs are capped at 384 threads, which
+// leaves 168 registers per thread.
+constexpr int kMaxThreadsGenWalk = 384;
+__host__ __device__ constexpr int max_cta_threads(bool gen, int nseg) {
+    return gen && nseg == 1 ? kMaxThreadsGenWalk : kMaxThreads;
+}
 
 struct PtTables {
     double beta[kMaxT];

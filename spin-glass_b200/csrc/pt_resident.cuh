@@ -86,7 +86,7 @@ __host__ __device__ constexpr int site_group(int zs, int cap) {
 }
 
 template <int L, bool GEN_H, int NSEG>
-__global__ void __launch_bounds__(kMaxThreads) pt_resident_kernel(const __grid_constant__ PtParams P) {
+__global__ void __launch_bounds__(max_cta_threads(GEN_H, NSEG)) pt_resident_kernel(const __grid_constant__ PtParams P) {
     using CF = Walk<L, NSEG>;
     constexpr int N = CF::N, NH = CF::NH, LH = CF::LH, PL = CF::PL, NC = CF::NC, ZS = CF::ZS;
     constexpr int TPQ = CF::TPQ;

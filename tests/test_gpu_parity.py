@@ -131,6 +131,15 @@ def test_tile_variants_match_oracle(csg, orc, L, T, qc, tpq, H):
     betas = orc.geometric_betas(T, 0.3, 2.0)
     spins, bonds = orc.init(L, W, C_, T, seed)
     csg.set_plan_override(qc, tpq)
+    if H != 0 and tpq == L * L // 2 and (qc * tpq + 31) // 32 * 32 > 384:
+        # the general-field kernel walking whole columns takes at most 384
+        # threads per CTA (168 registers each): the tile is refused, not run
+        try:
+            with pytest.raises(csg.CsgError, match="plan override exceeds device limits"):
+                csg.query_plan(L, W, C_, betas, H=H)
+        finally:
+            csg.set_plan_override(None)
+        return
     try:
         plan = csg.query_plan(L, W, C_, betas, H=H)
         assert (plan.quads_per_cta, plan.threads_per_quad) == (qc, tpq)
