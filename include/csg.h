@@ -210,7 +210,10 @@ int csg_query_plan(const csg_config* cfg, csg_plan* out);
 /* Force quads_per_cta (must divide n_copies*n_temps/4) and/or
  * threads_per_quad (L * L/2 * s for a built column split s) for later launches
  * of the resident kernel; a zero field keeps that part automatic, NULL
- * restores the automatic plan. */
+ * restores the automatic plan.  A CTA takes at most 512 threads, and at most
+ * 384 when H != 0 with threads_per_quad = L * L/2 (the general-field kernel
+ * walking whole columns, built for 168 registers per thread); a forced tile
+ * beyond that makes the launch fail with CSG_ERR_UNSUPPORTED. */
 int csg_set_plan_override(const csg_plan* plan);
 
 /* No counterpart in the reference.  The observable records of
