@@ -213,7 +213,8 @@ int csg_query_plan(const csg_config* cfg, csg_plan* out);
  * restores the automatic plan.  A CTA takes at most 512 threads, and at most
  * 384 when H != 0 with threads_per_quad = L * L/2 (the general-field kernel
  * walking whole columns, built for 168 registers per thread); a forced tile
- * beyond that makes the launch fail with CSG_ERR_UNSUPPORTED. */
+ * beyond that is refused with CSG_ERR_UNSUPPORTED by engine creation, plan
+ * queries and runs. */
 int csg_set_plan_override(const csg_plan* plan);
 
 /* No counterpart in the reference.  The observable records of
