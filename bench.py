@@ -71,11 +71,12 @@ def engine_flags(csg, args) -> int:
 
 
 def workload_config(n_gpus: int, swap_every: int = 1, measure_every: int = 1,
-                    engine: str = "auto", field: float = 0.0) -> dict:
+                    engine: str = "auto", field: float = 0.0,
+                    sweeps_per_step: int = SWEEPS_PER_STEP) -> dict:
     name = "plain PT engine, production size" + (" (streaming engine)" if engine == "stream" else "")
     return {"workload": name, "L": L, "samples": 32 * W,
             "copies": NCOPY, "temperatures": T, "T_range": [T_MIN, T_MAX],
-            "sweeps_per_step": SWEEPS_PER_STEP, "swap_every": swap_every,
+            "sweeps_per_step": sweeps_per_step, "swap_every": swap_every,
             "measure_every": measure_every,
             "field_H": field, "l2": "flushed between timed steps (256 MiB write)",
             "parallelism": f"sample shards x{n_gpus}"}
@@ -369,7 +370,7 @@ def run_ours(args, rank: int, world: int, dist) -> None:
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic (seeded +-J disorder, uniform random initial spins)",
             "config": workload_config(world, args.swap_every, args.measure_every, args.engine,
-                                      args.field),
+                                      args.field, args.sweeps_per_step),
             "roofline": {"bound": "int", "achieved": achieved / 1e12, "peak": peak["ops_per_s"] / 1e12,
                          "unit": "Tops/s (32-bit integer logic)",
                          "frac": achieved / peak["ops_per_s"], "traffic": profile_traffic(),
