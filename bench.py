@@ -70,14 +70,26 @@ def engine_flags(csg, args) -> int:
     return csg.CSG_ENGINE_STREAM if getattr(args, "engine", "auto") == "stream" else 0
 
 
+def stream_launches(sweep0: int, n: int, sps: int, spm: int) -> int:
+    """Kernel launches of n sweeps of the streaming engine's default path (two
+    colour launches per sweep; after a sweep that exchanges or measures, the
+    decisions, one exchange and/or overlap pass, and the measurement)."""
+    total = 0
+    for s in range(sweep0, sweep0 + n):
+        swap = sps > 0 and (s + 1) % sps == 0
+        meas = spm > 0 and (s + 1) % spm == 0
+        total += 2 + (1 if swap or meas else 0) + (1 if swap or meas else 0) + (1 if meas else 0)
+    return total
+
+
 def workload_config(n_gpus: int, swap_every: int = 1, measure_every: int = 1,
-                    engine: str = "auto", field: float = 0.0,
-                    sweeps_per_step: int = SWEEPS_PER_STEP) -> dict:
+                    engine: str = "auto", field: float = 0.0) -> dict:
+    """The production workload; a line reports its own step size beside it
+    (sweeps_per_step), so that both arms share this config."""
     name = "plain PT engine, production size" + (" (streaming engine)" if engine == "stream" else "")
     return {"workload": name, "L": L, "samples": 32 * W,
             "copies": NCOPY, "temperatures": T, "T_range": [T_MIN, T_MAX],
-            "sweeps_per_step": sweeps_per_step, "swap_every": swap_every,
-            "measure_every": measure_every,
+            "swap_every": swap_every, "measure_every": measure_every,
             "field_H": field, "l2": "flushed between timed steps (256 MiB write)",
             "parallelism": f"sample shards x{n_gpus}"}
 
@@ -369,18 +381,20 @@ def run_ours(args, rank: int, world: int, dist) -> None:
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic (seeded +-J disorder, uniform random initial spins)",
+            "sweeps_per_step": args.sweeps_per_step,
             "config": workload_config(world, args.swap_every, args.measure_every, args.engine,
-                                      args.field, args.sweeps_per_step),
+                                      args.field),
             "roofline": {"bound": "int", "achieved": achieved / 1e12, "peak": peak["ops_per_s"] / 1e12,
                          "unit": "Tops/s (32-bit integer logic)",
                          "frac": achieved / peak["ops_per_s"], "traffic": profile_traffic(),
                          "ops_per_attempt": OPS_PER_WORD_UPDATE / 32, "peak_source": peak["source"]},
             "e2e": {"value": e2e["value"], "unit": METRIC,
                     "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]},
-            # resident kernel: one launch per 1024-sweep step; streaming engine
-            # at L=16: four per sweep (fused sweep, decisions, exchange with
-            # overlaps, measurement)
-            "gpu_launches": args.steps * (args.sweeps_per_step * 4 if args.engine == "stream" else 1),
+            # resident kernel: one launch per step; streaming engine: its
+            # colour launches and exchange / measurement passes of every sweep
+            "gpu_launches": args.steps * (
+                stream_launches(SWEEP0, args.sweeps_per_step, args.swap_every, args.measure_every)
+                if args.engine == "stream" else 1),
             "exchange_boundary_cases": boundary,
             "clocks": clk.summary()}
     if world == 1 and not args.no_cpu_baseline:
@@ -647,7 +661,8 @@ def measure_production(csg, torch, dev, stream, flush, args) -> dict:
                                  SWEEP0 + k * SWEEPS_PER_STEP, SWEEPS_PER_STEP, stream.cuda_stream))
     att = args.steps * SWEEPS_PER_STEP * attempts_per_sweep()
     peak = int_peak_ops()
-    out = {"config": workload_config(1), "value": att / (t_ms * 1e6),
+    out = {"config": workload_config(1), "sweeps_per_step": SWEEPS_PER_STEP,
+           "value": att / (t_ms * 1e6),
            "ms_per_step": t_ms / args.steps,
            "roofline": int_roofline(SWEEPS_PER_STEP * W * NCOPY * T * N, per, peak),
            "plan": {"quads_per_cta": plan.quads_per_cta, "ctas_per_word": plan.ctas_per_word,
