@@ -248,21 +248,28 @@ def run(sim_dir: str, h_arg: str, *, group=None, engine_factory=None, log_dir: s
         out = step(lambda: open(base + "obs.bin", "ab") if lead else None)
         spfile, sbmeas = st["SPFILE"], st["SBMEAS"]
         t0 = time.perf_counter()
-        # run only queues the section on the GPU; the records of a section are
-        # taken before the next one is queued, and written while it runs
+
+        def write(rec):
+            out.write(np.ascontiguousarray(rec, np.float32).tobytes())
+            out.flush()
+
+        # run only queues a section on the GPU.  Each step takes a section's
+        # records and queues the next section before the collectives, and
+        # rank 0 writes the previous section's records while the GPU works.
         step(lambda: sh.run(sbmeas))
+        prev = None
         for done in range(0, spfile, sbmeas):
             log.progress(100.0 * done / spfile)
-            rec = sh.gather_rows(step(sh.engine.obs_records))
 
-            def next_and_write():
+            def take(prev=prev, done=done):
+                if lead and prev is not None:
+                    write(prev)
+                rec = sh.engine.obs_records()
                 if done + sbmeas < spfile:
                     sh.run(sbmeas)
-                if lead:
-                    out.write(np.ascontiguousarray(rec, np.float32).tobytes())
-                    out.flush()
-            step(next_and_write)
-        step(lambda: out.close() if lead else None)
+                return rec
+            prev = sh.gather_rows(step(take))
+        step(lambda: (write(prev), out.close()) if lead else None)
         secs = time.perf_counter() - t0
         t_e = secs * 1e12 / (spfile * N * 2 * st["NDIS"] * st["NREP"])
         log.record(f"t_e = {t_e:07.4f} ps")
