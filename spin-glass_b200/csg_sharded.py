@@ -181,13 +181,13 @@ def run(sim_dir: str, h_arg: str, *, group=None, engine_factory=None, log_dir: s
 
     def step(fn):
         """fn() on every rank, then agreement; its result on success."""
-        out, err = None, None
+        res, err = None, None
         try:
-            out = fn()
+            res = fn()
         except Exception as e:  # noqa: BLE001 - any local failure ends every rank
             err = e if str(e) else type(e).__name__
         agree(err)
-        return out
+        return res
 
     try:
         H = parse_field(h_arg)
@@ -257,19 +257,19 @@ def run(sim_dir: str, h_arg: str, *, group=None, engine_factory=None, log_dir: s
         # records and queues the next section before the collectives, and
         # rank 0 writes the previous section's records while the GPU works.
         step(lambda: sh.run(sbmeas))
-        prev = None
+        last = None  # records of the previous section (rank 0)
         for done in range(0, spfile, sbmeas):
             log.progress(100.0 * done / spfile)
 
-            def take(prev=prev, done=done):
-                if lead and prev is not None:
-                    write(prev)
+            def take(last=last, done=done):
+                if lead and last is not None:
+                    write(last)
                 rec = sh.engine.obs_records()
                 if done + sbmeas < spfile:
                     sh.run(sbmeas)
                 return rec
-            prev = sh.gather_rows(step(take))
-        step(lambda: (write(prev), out.close()) if lead else None)
+            last = sh.gather_rows(step(take))
+        step(lambda: (write(last), out.close()) if lead else None)
         secs = time.perf_counter() - t0
         t_e = secs * 1e12 / (spfile * N * 2 * st["NDIS"] * st["NREP"])
         log.record(f"t_e = {t_e:07.4f} ps")
