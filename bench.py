@@ -175,8 +175,10 @@ def profile_traffic(name: str = "pt_resident_L16_production"):
 
 
 def cpu_sample(target_s: float, n_threads: int = 0) -> dict:
-    """The CPU oracle (a scalar port of the reference's update rule, OpenMP over
-    planes) on the same workload, for a bounded number of sweeps."""
+    """The CPU oracle's multispin restatement of the reference's update rule
+    (all 32 samples of a word at once, OpenMP over words, copies and
+    temperature quads; bit-identical to the per-sample oracle) on the same
+    workload, for a bounded number of sweeps."""
     from oracle import oracle as orc
     orc.build()
     betas = 1.0 / (T_MIN * (T_MAX / T_MIN) ** (np.arange(T) / (T - 1)))
@@ -185,7 +187,8 @@ def cpu_sample(target_s: float, n_threads: int = 0) -> dict:
     sweeps, t0 = 0, time.perf_counter()
     while True:
         orc.run(spins, bonds, L=L, betas=betas, H=0.0, seed=SEED, sweep0=SWEEP0 + sweeps,
-                n_sweeps=1, sweeps_per_swap=1, sweeps_per_meas=1, obs=obs, n_threads=n_threads)
+                n_sweeps=1, sweeps_per_swap=1, sweeps_per_meas=1, obs=obs, n_threads=n_threads,
+                multispin=True)
         sweeps += 1
         el = time.perf_counter() - t0
         if el >= target_s:
@@ -194,7 +197,8 @@ def cpu_sample(target_s: float, n_threads: int = 0) -> dict:
     return {"value": sweeps * attempts_per_sweep() / (el * 1e9), "unit": METRIC, "cores": cores,
             "kind": "port",
             "sample": f"{sweeps} full sweeps (+exchange, +measurement) of the same workload, "
-                      f"{el:.1f} s, {cores} OpenMP threads"}
+                      f"{el:.1f} s, {cores} OpenMP threads; multispin CPU restatement "
+                      "(32 samples per word, bit-sliced)"}
 
 
 def _t_e(text: str):
@@ -281,7 +285,7 @@ def run_reference(args, rank: int, world: int) -> None:
         for m, sps, spm, s_, b_, o_ in sims:
             orc.run(s_, b_, L=m["L"], betas=m["betas"], H=0.0, seed=m["seed"],
                     sweep0=SWEEP0 + k * step_sweeps, n_sweeps=step_sweeps, sweeps_per_swap=sps,
-                    sweeps_per_meas=spm, obs=o_)
+                    sweeps_per_meas=spm, obs=o_, multispin=True)
 
     for k in range(args.warmup):
         step(k)
@@ -292,7 +296,8 @@ def run_reference(args, rank: int, world: int) -> None:
     value = args.steps * step_sweeps * words * 32 / (el * 1e9)
     sample = (f"{args.steps} steps of {step_sweeps} sweep(s) of every member of the workload, "
               f"{cores} OpenMP threads; the reference itself has no CPU implementation of "
-              "this path, so its update rule runs as restated by the oracle")
+              "this path, so its update rule runs as restated by the oracle, 32 samples "
+              "per word at once (bit-identical to the per-sample oracle)")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": el * 1e3 / args.steps, "sweeps_per_step": step_sweeps,
@@ -603,9 +608,10 @@ def int_roofline(words_per_launch: float, per_launch_ms: list, peak: dict) -> di
 
 
 def cpu_sample_mixed(target_s: float, sps: int, spm: int) -> dict:
-    """The CPU oracle (a scalar port of the reference's update rule, OpenMP
-    over planes, all host cores) on the mixed workload's members, for a
-    bounded number of sweeps."""
+    """The CPU oracle's multispin restatement of the reference's update rule
+    (all 32 samples of a word at once, OpenMP over words, copies and
+    temperature quads, all host cores; bit-identical to the per-sample oracle)
+    on the mixed workload's members, for a bounded number of sweeps."""
     from oracle import oracle as orc
     orc.build()
     state = []
@@ -619,7 +625,7 @@ def cpu_sample_mixed(target_s: float, sps: int, spm: int) -> dict:
             for m, s_, b_, o_ in state:
                 orc.run(s_, b_, L=m["L"], betas=m["betas"], H=0.0, seed=m["seed"],
                         sweep0=SWEEP0 + sweeps, n_sweeps=16, sweeps_per_swap=sps,
-                        sweeps_per_meas=spm, obs=o_, n_threads=n_threads)
+                        sweeps_per_meas=spm, obs=o_, n_threads=n_threads, multispin=True)
             sweeps += 16
             el = time.perf_counter() - t0
             if el >= seconds:
@@ -630,7 +636,8 @@ def cpu_sample_mixed(target_s: float, sps: int, spm: int) -> dict:
     out = {"value": sweeps * MIXED_WORDS_PER_SWEEP * 32 / (el * 1e9), "unit": METRIC,
            "cores": cores, "kind": "port",
            "sample": f"{sweeps} sweeps of every member of the same workload and schedule, "
-                     f"{el:.1f} s, {cores} OpenMP threads"}
+                     f"{el:.1f} s, {cores} OpenMP threads; multispin CPU restatement "
+                     "(32 samples per word, bit-sliced)"}
     # one host thread beside it, a shorter sample
     s1, e1 = sample(target_s / 4, 1)
     out["one_thread"] = {"value": s1 * MIXED_WORDS_PER_SWEEP * 32 / (e1 * 1e9), "cores": 1,

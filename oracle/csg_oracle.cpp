@@ -161,6 +161,85 @@ void add_u128(uint64_t* acc, uint64_t lo, uint64_t hi) {
     acc[1] += hi + (acc[0] < old ? 1u : 0u);
 }
 
+// ---------------------------------------------------------------------------
+// The multispin restatement (timing baseline, checked equal to the
+// per-sample loop of run_impl by the tests).  It evaluates the same rule for
+// all 32 samples of a word at once, as the reference's own kernel does for its
+// 24 temperatures (SWAR counts, eamsim.cu:173-180): the unsatisfied-bond count
+// U of every sample as three bit-slices, then, per class (centre bit s, U),
+// the samples of that class when the draw is below thr[s][U].
+// ---------------------------------------------------------------------------
+
+uint32_t accept_all(const uint32_t u[6], uint32_t s0, uint32_t r, const uint64_t* thr /* [2][7] */) {
+    const uint32_t sa = u[0] ^ u[1] ^ u[2], ca = (u[0] & u[1]) | (u[2] & (u[0] ^ u[1]));
+    const uint32_t sb = u[3] ^ u[4] ^ u[5], cb = (u[3] & u[4]) | (u[5] & (u[3] ^ u[4]));
+    // U = sa + sb + 2 (ca + cb) = b0 + 2 (c0 + ca + cb) = b0 + 2 b1 + 4 b2
+    const uint32_t b0 = sa ^ sb, c0 = sa & sb;
+    const uint32_t b1 = ca ^ cb ^ c0, b2 = (ca & cb) | (c0 & (ca ^ cb));
+    uint32_t acc = 0;
+    for (int U = 0; U <= 6; ++U) {
+        const uint32_t eq = ((U & 1) ? b0 : ~b0) & ((U & 2) ? b1 : ~b1) & ((U & 4) ? b2 : ~b2);
+        if ((uint64_t)r < thr[U]) acc |= eq & ~s0;
+        if ((uint64_t)r < thr[7 + U]) acc |= eq & s0;
+    }
+    return acc;
+}
+
+// Neighbour slots (-x, +x, -y, +y, -z, +z) and the site index of every slot.
+struct Neighbours {
+    std::vector<int32_t> nb, site;
+    explicit Neighbours(const Geo& g) : nb((size_t)g.N * 6), site((size_t)g.N) {
+        for (int z = 0; z < g.L; ++z)
+            for (int y = 0; y < g.L; ++y)
+                for (int x = 0; x < g.L; ++x) {
+                    const int64_t si = g.slot(x, y, z);
+                    site[si] = (int32_t)g.site(x, y, z);
+                    const int64_t n[6] = {g.slot(g.wrap(x - 1), y, z), g.slot(g.wrap(x + 1), y, z),
+                                          g.slot(x, g.wrap(y - 1), z), g.slot(x, g.wrap(y + 1), z),
+                                          g.slot(x, y, g.wrap(z - 1)), g.slot(x, y, g.wrap(z + 1))};
+                    for (int k = 0; k < 6; ++k) nb[(size_t)si * 6 + k] = (int32_t)n[k];
+                }
+    }
+};
+
+// Sweep s of every (word, copy, quad), colour 0 then colour 1: the sites,
+// draws and thresholds of the per-sample loop; sites of one colour are
+// independent, so their order does not matter.
+void sweep_multispin(const orc_params* p, const Dims& D, const Neighbours& G, uint32_t* spins,
+                     const uint32_t* bonds, int64_t s, int nthr) {
+    const int64_t NH = D.g.NH;
+    const int W = D.W, C = D.C, Q = D.Q;
+    for (int phase = 0; phase < 2; ++phase) {
+#pragma omp parallel for collapse(3) schedule(static) num_threads(nthr)
+        for (int w = 0; w < W; ++w)
+            for (int c = 0; c < C; ++c)
+                for (int q = 0; q < Q; ++q) {
+                    const uint32_t ctr3 = kTagSweep | ((uint32_t)c << 8) | (uint32_t)q;
+                    const uint32_t* Jx = bonds + D.bond(w, 0, 0);
+                    const uint32_t* Jy = bonds + D.bond(w, 1, 0);
+                    const uint32_t* Jz = bonds + D.bond(w, 2, 0);
+                    uint32_t* S = spins + D.spin(w, c, 4 * q, 0);  // S[slot * 4 + k]
+                    const uint64_t* thr = p->thr + (size_t)(4 * q) * 14;
+                    for (int64_t si = phase * NH; si < (phase + 1) * NH; ++si) {
+                        const int32_t* nb = &G.nb[(size_t)si * 6];
+                        const uint32_t J[6] = {Jx[nb[0]], Jx[si], Jy[nb[2]], Jy[si], Jz[nb[4]], Jz[si]};
+                        uint32_t r[4];
+                        philox_ctr((uint32_t)G.site[si], (uint32_t)s, (uint32_t)(w + p->word0), ctr3,
+                                   p->seed, r);
+                        for (int k = 0; k < 4; ++k) {
+                            const uint32_t s0 = S[si * 4 + k];
+                            uint32_t u[6];
+                            for (int n = 0; n < 6; ++n) u[n] = s0 ^ S[(size_t)nb[n] * 4 + k] ^ J[n];
+                            S[si * 4 + k] = s0 ^ accept_all(u, s0, r[k], thr + (size_t)k * 14);
+                        }
+                    }
+                }
+    }
+}
+
+int run_impl(const orc_params* p, uint32_t* spins, const uint32_t* bonds, int64_t sweep0,
+             int64_t n_sweeps, orc_obs* obs, bool multispin);
+
 }  // namespace
 
 extern "C" {
@@ -251,6 +330,20 @@ int orc_overlaps(int32_t L, int32_t W, int32_t T, const uint32_t* spins, int32_t
 // (eamsim.cu:184-195).  One 32-bit draw serves the 32 samples of a word.
 int orc_run(const orc_params* p, uint32_t* spins, const uint32_t* bonds, int64_t sweep0,
             int64_t n_sweeps, orc_obs* obs) {
+    return run_impl(p, spins, bonds, sweep0, n_sweeps, obs, false);
+}
+
+int orc_run_multispin(const orc_params* p, uint32_t* spins, const uint32_t* bonds, int64_t sweep0,
+                      int64_t n_sweeps, orc_obs* obs) {
+    return run_impl(p, spins, bonds, sweep0, n_sweeps, obs, true);
+}
+
+}  // extern "C"
+
+namespace {
+
+int run_impl(const orc_params* p, uint32_t* spins, const uint32_t* bonds, int64_t sweep0,
+             int64_t n_sweeps, orc_obs* obs, bool multispin) {
     if (!p || !spins || !bonds || !p->betas || !p->thr || n_sweeps < 0) return 1;
     if (!dims_ok(p->L, p->W, p->C, p->T)) return 1;
     const Dims D(p->L, p->W, p->C, p->T);
@@ -259,9 +352,12 @@ int orc_run(const orc_params* p, uint32_t* spins, const uint32_t* bonds, int64_t
     const int nthr = threads_for(p);
     std::vector<int32_t> E((size_t)W * C * T * 32), M((size_t)W * C * T * 32);
     std::vector<int32_t> Dq((size_t)W * T * 32);
+    std::vector<Neighbours> G;
+    if (multispin) G.emplace_back(g);
 
     for (int64_t s = sweep0; s < sweep0 + n_sweeps; ++s) {
-        for (int phase = 0; phase < 2; ++phase) {
+        if (multispin) sweep_multispin(p, D, G[0], spins, bonds, s, nthr);
+        for (int phase = 0; phase < 2 && !multispin; ++phase) {
 #pragma omp parallel for collapse(3) schedule(static) num_threads(nthr)
             for (int w = 0; w < W; ++w)
                 for (int c = 0; c < C; ++c)
@@ -410,6 +506,10 @@ int orc_run(const orc_params* p, uint32_t* spins, const uint32_t* bonds, int64_t
     }
     return 0;
 }
+
+}  // namespace
+
+extern "C" {
 
 // Observable records of eamsim.cuh:55-62 for the current state.  e and m
 // follow the float arithmetic of eamsim.cu:320-325 and :413-414; q_0 and

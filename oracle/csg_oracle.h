@@ -81,6 +81,13 @@ int orc_init(int32_t L, int32_t W, int32_t C, int32_t T, uint64_t seed, int32_t 
 int orc_run(const orc_params* p, uint32_t* spins, const uint32_t* bonds,
             int64_t sweep0, int64_t n_sweeps, orc_obs* obs);
 
+/* orc_run with the Metropolis step evaluated for all 32 samples of a word at
+ * once (bit-sliced bond counts, a mask per acceptance class) instead of one
+ * sample at a time: the CPU timing baseline.  Same arguments, same results
+ * bit for bit (checked by the tests); exchange and measurement are shared. */
+int orc_run_multispin(const orc_params* p, uint32_t* spins, const uint32_t* bonds,
+                      int64_t sweep0, int64_t n_sweeps, orc_obs* obs);
+
 /* Bond energy E_b = -(sum of J s s) and magnetisation per sample, per plane:
  * e[W][C][T][32], m[W][C][T][32]. */
 int orc_energies(int32_t L, int32_t W, int32_t C, int32_t T,

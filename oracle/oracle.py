@@ -66,12 +66,14 @@ def lib():
         L.orc_thresholds.argtypes = [C.c_int32, vp, C.c_double, vp]
         L.orc_init.argtypes = [C.c_int32] * 4 + [C.c_uint64, C.c_int32, vp, vp]
         L.orc_run.argtypes = [C.POINTER(Params), vp, vp, C.c_int64, C.c_int64, C.POINTER(Obs)]
+        L.orc_run_multispin.argtypes = L.orc_run.argtypes
         L.orc_energies.argtypes = [C.c_int32] * 4 + [vp, vp, vp, vp]
         L.orc_overlaps.argtypes = [C.c_int32] * 3 + [vp, vp, vp]
         L.orc_obs_records.argtypes = [C.c_int32] * 3 + [C.c_float, vp, vp, vp]
         L.orc_to_ref_lattice.argtypes = [C.c_int32] * 3 + [vp, vp, vp]
         L.orc_from_ref_lattice.argtypes = [C.c_int32] * 3 + [vp, vp, vp]
-        for f in ("orc_thresholds", "orc_init", "orc_run", "orc_energies", "orc_overlaps",
+        for f in ("orc_thresholds", "orc_init", "orc_run", "orc_run_multispin", "orc_energies",
+                  "orc_overlaps",
                   "orc_obs_records", "orc_to_ref_lattice", "orc_from_ref_lattice"):
             getattr(L, f).restype = C.c_int
         _lib = L
@@ -157,7 +159,10 @@ class Observables:
 def run(spins: np.ndarray, bonds: np.ndarray, *, L: int, betas, H: float, seed: int,
         sweep0: int, n_sweeps: int, sweeps_per_swap: int = 1, sweeps_per_meas: int = 0,
         meas_start: int = 0, obs: Observables | None = None, n_threads: int = 0,
-        word0: int = 0) -> Observables:
+        word0: int = 0, multispin: bool = False) -> Observables:
+    """n_sweeps sweeps from global sweep sweep0.  multispin: the Metropolis
+    step for all 32 samples of a word at once (orc_run_multispin, the timing
+    baseline); the default is the one-sample-at-a-time restatement."""
     W, C_, Q = spins.shape[:3]
     T = 4 * Q
     b = np.ascontiguousarray(betas, dtype=np.float64)
@@ -168,8 +173,8 @@ def run(spins: np.ndarray, bonds: np.ndarray, *, L: int, betas, H: float, seed: 
                sweeps_per_meas=sweeps_per_meas, meas_start=meas_start, H=float(H),
                seed=seed, betas=_p(b).value, thr=_p(thr).value, n_threads=n_threads,
                word0=word0)
-    _check(lib().orc_run(C.byref(p), _p(spins), _p(bonds), sweep0, n_sweeps, C.byref(obs.c)),
-           "run")
+    fn = lib().orc_run_multispin if multispin else lib().orc_run
+    _check(fn(C.byref(p), _p(spins), _p(bonds), sweep0, n_sweeps, C.byref(obs.c)), "run")
     return obs
 
 

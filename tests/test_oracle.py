@@ -139,3 +139,36 @@ def test_high_temperature_energy_matches_reference_table(orc):
         per_sample = e[:, :, [k, k + 2], :].mean(axis=(1, 2)).ravel()
         mean, err = per_sample.mean(), per_sample.std(ddof=1) / np.sqrt(per_sample.size)
         assert abs(mean - r[5]) < 5 * err + 1e-4, (r[0], mean, r[5], err)
+
+
+_OBS_FIELDS = ("e_sum", "m_sum", "q_sum", "q2_sum", "q4_sum", "hist", "e_last", "m_last",
+               "d_last", "swap_acc", "swap_log")
+
+
+@pytest.mark.parametrize("L,W,C_,T,H,sps,spm,word0", [
+    (4, 1, 2, 4, 0.0, 1, 1, 0),
+    (6, 2, 2, 8, 0.1875, 1, 1, 3),
+    (8, 1, 1, 12, 1.5, 2, 3, 0),
+    (10, 1, 2, 8, 2.5, 1, 2, 0),
+    (12, 1, 2, 16, 4.0, 16, 1024, 7),
+])
+def test_multispin_run_equals_the_per_sample_restatement(orc, L, W, C_, T, H, sps, spm, word0):
+    """orc_run_multispin (the CPU timing baseline: all 32 samples of a word at
+    once) gives the per-sample restatement's bits: spins and every
+    observable, with exchanges and measurements, at zero and non-zero field."""
+    betas = orc.geometric_betas(T, 0.3, 2.0)
+    n = 24
+    out = []
+    for multispin in (False, True):
+        spins, bonds = orc.init(L, W, C_, T, 99 + L, word0)
+        obs = orc.Observables(L, W, C_, T, log_rounds=n)
+        orc.run(spins, bonds, L=L, betas=betas, H=H, seed=99 + L, sweep0=5, n_sweeps=n,
+                sweeps_per_swap=sps, sweeps_per_meas=spm, obs=obs, word0=word0,
+                multispin=multispin)
+        out.append((spins, obs))
+    (s0, o0), (s1, o1) = out
+    np.testing.assert_array_equal(s1, s0)
+    for f in _OBS_FIELDS:
+        np.testing.assert_array_equal(getattr(o1, f), getattr(o0, f), err_msg=f)
+    assert (o1.n_meas, o1.swap_rounds, o1.boundary) == (o0.n_meas, o0.swap_rounds, o0.boundary)
+    assert o0.n_meas > 0 or spm > n
