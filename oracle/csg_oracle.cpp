@@ -4,6 +4,9 @@
 // It deliberately shares no code with the CUDA engine: its Philox, its
 // indexing and its acceptance test are written out here on their own so that
 // a bit-exact match between the two is evidence, not a tautology.
+// orc_run_multispin, the CPU timing baseline, replaces only the per-sample
+// acceptance loop by one evaluated for the 32 samples of a word at once; the
+// tests check that the two give the same bits.
 #include "csg_oracle.h"
 
 #include <cmath>

@@ -17,7 +17,9 @@
  *   - bond generation / per-site bond bits   eamsim.cu:578-619
  *   - beta ladder                            eamsim.cu:725-744
  * The random numbers come from its own Philox4x32-10 (Salmon et al., SC'11),
- * written independently of the engine's copy.
+ * written independently of the engine's copy.  orc_run_multispin (the CPU
+ * timing baseline) evaluates the acceptance of the 32 samples of a word at
+ * once and is checked against the per-sample orc_run.
  *
  * Layout (identical to the engine's canonical host layout):
  *   spins  uint32 [W][C][T/4][N][4]   site index = checkerboard slot, last
