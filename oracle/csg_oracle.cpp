@@ -173,17 +173,47 @@ void add_u128(uint64_t* acc, uint64_t lo, uint64_t hi) {
 // the samples of that class when the draw is below thr[s][U].
 // ---------------------------------------------------------------------------
 
-uint32_t accept_all(const uint32_t u[6], uint32_t s0, uint32_t r, const uint64_t* thr /* [2][7] */) {
-    const uint32_t sa = u[0] ^ u[1] ^ u[2], ca = (u[0] & u[1]) | (u[2] & (u[0] ^ u[1]));
-    const uint32_t sb = u[3] ^ u[4] ^ u[5], cb = (u[3] & u[4]) | (u[5] & (u[3] ^ u[4]));
+// The four temperature planes of a quad side by side, one per lane.
+typedef uint32_t v4u __attribute__((vector_size(16)));
+
+inline v4u load4(const uint32_t* a) {
+    v4u v;
+    std::memcpy(&v, a, sizeof v);
+    return v;
+}
+inline void store4(uint32_t* a, v4u v) { std::memcpy(a, &v, sizeof v); }
+inline v4u splat(uint32_t x) { return v4u{x, x, x, x}; }
+
+// Thresholds thr[t][s][U] of a quad's 4 planes (lane k = plane 4q+k) as
+// 32-bit lanes: r < thr  <=>  r < lo || always, where always marks thr = 2^32.
+struct QuadThresholds {
+    v4u lo[2][7], always[2][7];
+    explicit QuadThresholds(const uint64_t* thr /* [4][2][7] */) {
+        for (int sb = 0; sb < 2; ++sb)
+            for (int U = 0; U < 7; ++U)
+                for (int k = 0; k < 4; ++k) {
+                    const uint64_t t = thr[(size_t)k * 14 + sb * 7 + U];
+                    lo[sb][U][k] = t >> 32 ? 0u : (uint32_t)t;
+                    always[sb][U][k] = t >> 32 ? 0xFFFFFFFFu : 0u;
+                }
+    }
+};
+
+// Accepted flips of the 32 samples of the 4 planes of a site: U of every
+// sample as three bit-slices from full adders, then the samples of every
+// class (centre bit, U) whose threshold the plane's draw is below.
+inline v4u accept_quad(const v4u u[6], v4u s0, v4u r, const QuadThresholds& th) {
+    const v4u sa = u[0] ^ u[1] ^ u[2], ca = (u[0] & u[1]) | (u[2] & (u[0] ^ u[1]));
+    const v4u sb = u[3] ^ u[4] ^ u[5], cb = (u[3] & u[4]) | (u[5] & (u[3] ^ u[4]));
     // U = sa + sb + 2 (ca + cb) = b0 + 2 (c0 + ca + cb) = b0 + 2 b1 + 4 b2
-    const uint32_t b0 = sa ^ sb, c0 = sa & sb;
-    const uint32_t b1 = ca ^ cb ^ c0, b2 = (ca & cb) | (c0 & (ca ^ cb));
-    uint32_t acc = 0;
+    const v4u b0 = sa ^ sb, c0 = sa & sb;
+    const v4u b1 = ca ^ cb ^ c0, b2 = (ca & cb) | (c0 & (ca ^ cb));
+    v4u acc = splat(0);
     for (int U = 0; U <= 6; ++U) {
-        const uint32_t eq = ((U & 1) ? b0 : ~b0) & ((U & 2) ? b1 : ~b1) & ((U & 4) ? b2 : ~b2);
-        if ((uint64_t)r < thr[U]) acc |= eq & ~s0;
-        if ((uint64_t)r < thr[7 + U]) acc |= eq & s0;
+        const v4u eq = ((U & 1) ? b0 : ~b0) & ((U & 2) ? b1 : ~b1) & ((U & 4) ? b2 : ~b2);
+        const v4u lt0 = (v4u)(r < th.lo[0][U]) | th.always[0][U];
+        const v4u lt1 = (v4u)(r < th.lo[1][U]) | th.always[1][U];
+        acc |= eq & ((lt0 & ~s0) | (lt1 & s0));
     }
     return acc;
 }
@@ -222,19 +252,17 @@ void sweep_multispin(const orc_params* p, const Dims& D, const Neighbours& G, ui
                     const uint32_t* Jy = bonds + D.bond(w, 1, 0);
                     const uint32_t* Jz = bonds + D.bond(w, 2, 0);
                     uint32_t* S = spins + D.spin(w, c, 4 * q, 0);  // S[slot * 4 + k]
-                    const uint64_t* thr = p->thr + (size_t)(4 * q) * 14;
+                    const QuadThresholds th(p->thr + (size_t)(4 * q) * 14);
                     for (int64_t si = phase * NH; si < (phase + 1) * NH; ++si) {
                         const int32_t* nb = &G.nb[(size_t)si * 6];
                         const uint32_t J[6] = {Jx[nb[0]], Jx[si], Jy[nb[2]], Jy[si], Jz[nb[4]], Jz[si]};
                         uint32_t r[4];
                         philox_ctr((uint32_t)G.site[si], (uint32_t)s, (uint32_t)(w + p->word0), ctr3,
                                    p->seed, r);
-                        for (int k = 0; k < 4; ++k) {
-                            const uint32_t s0 = S[si * 4 + k];
-                            uint32_t u[6];
-                            for (int n = 0; n < 6; ++n) u[n] = s0 ^ S[(size_t)nb[n] * 4 + k] ^ J[n];
-                            S[si * 4 + k] = s0 ^ accept_all(u, s0, r[k], thr + (size_t)k * 14);
-                        }
+                        const v4u s0 = load4(S + si * 4);
+                        v4u u[6];
+                        for (int n = 0; n < 6; ++n) u[n] = s0 ^ load4(S + (size_t)nb[n] * 4) ^ splat(J[n]);
+                        store4(S + si * 4, s0 ^ accept_quad(u, s0, v4u{r[0], r[1], r[2], r[3]}, th));
                     }
                 }
     }
