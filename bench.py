@@ -11,8 +11,9 @@ schedule, the plain engine looping over the same lattices (both schedules),
 the end-to-end rate through the csg_batch_* API with host state in and
 observables out, the production shape (L=16, 1024 samples, 24 temperatures,
 exchange and measurement every sweep), a short serving run (p50/p99 against a
-stated p99 objective), the CPU oracle on the host cores, and the reference's
-own CUDA program on this GPU.
+stated p99 objective), the CPU oracle on the host cores (its multispin
+restatement, 32 samples per word at once, bit-identical to the per-sample
+oracle), and the reference's own CUDA program on this GPU.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--workload mixed|production|serving|large]
